@@ -1,0 +1,329 @@
+"""Benchmark of the streaming k-mer table's hot path on B200: k-mers/s of upsert + find.
+
+Workload (one step): a map <31, u64, 22> sized for n = 10M keys, emptied, then upsert(c + 1, init 1) of 333,333 reads
+of 150 bp (10x over a seeded 5 Mbp genome, 50 % reverse-complemented, 0.5 % substitutions, 0.05 % N), then a
+per-position lookup (found + value) of 1M held-out reads of the same model. Unit: k-mer positions per second over
+both phases (40.0M + 120.0M positions). Synthetic data stands in for the reference's read sets.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+
+`value` times the device-resident path (reads already in HBM, kache_b200_upsert_dev / kache_b200_lookup_dev);
+`e2e` times the C interface with host buffers (kache_insert / kache_lookup: gather + H2D + kernels + D2H of the
+per-position results). With N > 1 each rank runs its own table on its own reads (weak scaling, no collective:
+tables are independent objects). `--impl reference` times the reference's own CPU table (oracle/_ref) on the same
+workload with all host threads.
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path[:0] = [ROOT, os.path.join(ROOT, "kache-hash_b200")]
+
+import numpy as np  # noqa: E402
+
+import synth  # noqa: E402
+
+METRIC = "k-mers/s upsert+find (config 1: <31,u64,22> n=10M, 333,333 x 150 bp upsert(c+1) + 1M held-out reads find)"
+N_KEYS = 10_000_000
+
+
+def load_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class Clocks:
+    """nvidia-smi samples during the timed region."""
+
+    def __init__(self, gpu_index):
+        self.rows, self.proc = [], None
+        self.gpu = gpu_index
+
+    def start(self):
+        q = "clocks.sm,clocks.max.sm,utilization.gpu,clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap"
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={q}", "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([x.strip() for x in line.split(",")])
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        rows = [r for r in self.rows if len(r) >= 7]
+        busy = [r for r in rows if r[2].isdigit() and int(r[2]) > 0] or rows
+        if not busy:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        sm = sorted(int(r[0]) for r in busy if r[0].isdigit())
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in busy for i in range(4) if r[3 + i].lower() == "active"})
+        return {"sm_mhz": sm[len(sm) // 2] if sm else None, "sm_max_mhz": int(busy[0][1]) if busy[0][1].isdigit() else None,
+                "reasons": reasons, "samples": len(busy)}
+
+
+def dist_env():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+def workload(rank):
+    g, ins, held = synth.config1()
+    if rank:
+        # Each rank its own reads of the same shape (weak scaling).
+        ins = synth.reads_fixed(g, 333_333, 150, seed=11 + 100 * rank)
+        held = synth.reads_fixed(g, 1_000_000, 150, seed=2 + 100 * rank)
+    return ins, held
+
+
+def positions(off, k=31):
+    lens = np.diff(off).astype(np.int64)
+    return int(np.maximum(lens - k + 1, 0).sum())
+
+
+def cpu_baseline_sample(ins, held, threads):
+    """The reference's own table (oracle/_ref) on a bounded sample of the same workload: a tenth of the upsert reads
+    into a table sized for a tenth of the keys, then counts over a tenth of the held-out reads."""
+    import oracle
+    L = oracle.ref()
+    if L is None:
+        return None
+    from kache import Batch
+    bi, bh = Batch(*ins), Batch(*held)
+    si, sh = bi.slice(0, bi.n // 10), bh.slice(0, bh.n // 10)
+    t = L.ref_new(0, N_KEYS // 10, 0.8, 0, threads)
+    out = oracle._u64()
+    t_up = L.ref_bench_upsert(t, si.bases.ctypes.data, si.off.ctypes.data, si.n, 64, threads, 16, 1, oracle.ctypes.byref(out))
+    t_q = L.ref_bench_count(t, sh.bases.ctypes.data, sh.off.ctypes.data, sh.n, 64, threads, oracle.ctypes.byref(out))
+    L.ref_free(t)
+    p = positions(si.off) + positions(sh.off)
+    return {"value": p / (t_up + t_q), "unit": "k-mers/s", "cores": threads, "kind": "reference",
+            "sample": f"upsert {si.n} reads + count {sh.n} held-out reads ({p} positions), batches of 64 reads, {threads} threads"}
+
+
+def run_reference(args):
+    ws, rank, _ = dist_env()
+    if rank != 0:
+        return
+    import oracle
+    L = oracle.ref()
+    if L is None:
+        print(json.dumps({"impl": "reference", "unavailable": "the reference's table (oracle/_ref) was not built on this machine"}))
+        return
+    from kache import Batch
+    ins, held = workload(0)
+    bi, bh = Batch(*ins), Batch(*held)
+    threads = min(128, os.cpu_count() or 1)
+    P = positions(bi.off) + positions(bh.off)
+    out = oracle._u64()
+    times = []
+    for s in range(args.warmup + args.steps):
+        t = L.ref_new(0, N_KEYS, 0.8, 0, threads)
+        t_up = L.ref_bench_upsert(t, bi.bases.ctypes.data, bi.off.ctypes.data, bi.n, 64, threads, 16, 1, oracle.ctypes.byref(out))
+        t_q = L.ref_bench_count(t, bh.bases.ctypes.data, bh.off.ctypes.data, bh.n, 64, threads, oracle.ctypes.byref(out))
+        L.ref_free(t)
+        if s >= args.warmup:
+            times.append(t_up + t_q)
+    T = sum(times)
+    v = P * args.steps / T
+    print(json.dumps({"impl": "reference", "metric": METRIC, "value": v, "unit": "k-mers/s", "n_gpus": ws, "steps": args.steps,
+                      "warmup": args.warmup, "ms_per_step": 1000 * T / args.steps, "higher_is_better": True, "scaling": "weak",
+                      "vs_baseline": None, "dtype": "u64", "data": "synthetic",
+                      "config": {"workload": "config 1: <31,u64,22> n=10M; upsert(c+1, init 1) 333,333 x 150 bp; find 1M x 150 bp held-out",
+                                 "upsert_positions": positions(bi.off), "find_positions": positions(bh.off), "find": "count per read"},
+                      "cpu_baseline": {"value": v, "unit": "k-mers/s", "cores": threads, "kind": "reference",
+                                       "sample": "the whole workload per step, batches of 64 reads round-robin over the threads"},
+                      "e2e": {"value": v, "unit": "k-mers/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}))
+
+
+def run_b200(args):
+    import torch
+    import kache
+    from kache import Batch
+    ws, rank, local = dist_env()
+    torch.cuda.set_device(local)
+    dist = None
+    if ws > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300))
+
+    ins, held = workload(rank)
+    bi, bh = Batch(*ins), Batch(*held)
+    P_up, P_find = positions(bi.off), positions(bh.off)
+    P = P_up + P_find
+    dev = torch.device("cuda", local)
+    stream = torch.cuda.current_stream()
+
+    d_ins_b = torch.from_numpy(bi.bases).to(dev)
+    d_ins_o = torch.from_numpy(bi.off.view(np.int64)).to(dev)
+    d_held_b = torch.from_numpy(bh.bases).to(dev)
+    d_held_o = torch.from_numpy(bh.off.view(np.int64)).to(dev)
+    d_found = torch.empty(P_find, dtype=torch.uint8, device=dev)
+    d_vals = torch.empty(P_find, dtype=torch.int64, device=dev)
+
+    T = kache.Table(31, 8, N_KEYS, 0.8, False)
+    T.set_stream(stream.cuda_stream)
+    u = T.register()
+
+    def step_dev():
+        T.clear()
+        T.upsert_dev(u, d_ins_b.data_ptr(), d_ins_o.data_ptr(), bi.n, kache.ADD_WRAP, 1, 1)
+        T.lookup_dev(d_held_b.data_ptr(), d_held_o.data_ptr(), bh.n, d_found.data_ptr(), d_vals.data_ptr(), None)
+
+    found_h = np.empty(P_find, np.uint8)
+    vals_h = np.empty(P_find, np.uint64)
+
+    def step_e2e():
+        T.clear()
+        kache.lib().kache_insert(T.h, u, *bi.args(), kache.ADD, 1, None)
+        kache.lib().kache_lookup(T.h, *bh.args(), found_h.ctypes.data, vals_h.ctypes.data, None)
+
+    def barrier():
+        torch.cuda.synchronize()
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def max_over_ranks(x):
+        if dist is None:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    # Device-resident: warm-up, then exactly `steps` steps between barriers, timed with CUDA events on the stream.
+    for _ in range(args.warmup):
+        step_dev()
+    barrier()
+    clocks = Clocks(local)
+    clocks.start()
+    time.sleep(0.3)
+    launches0 = kache.kernel_launches()
+    T.profile(True)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        step_dev()
+    e1.record(stream)
+    barrier()
+    ms = max_over_ranks(e0.elapsed_time(e1)) / args.steps
+    launches = kache.kernel_launches() - launches0
+    prof = {kind: T.profile_read(i) for i, kind in enumerate(["upsert", "update", "lookup", "reduce", "resize", "other"])}
+    T.profile(False)
+    clk = clocks.stop()
+
+    # Per-kernel roofline: algorithmic bytes per launch over the kernel's mean event-timed duration.
+    st = T.stats()
+    inserted = T.size()
+    fh = d_found.cpu().numpy()
+    hit = float((fh == 1).sum()) / max(1, P_find)
+    rho = run_density(kache, bi.slice(0, 5000)) if rank == 0 else 0.0
+    b_in_up = float(bi.off[-1]) / P_up
+    b_in_find = float(bh.off[-1]) / P_find
+    A_up = b_in_up + 32 * rho + 32 * (1 - inserted / P_up) + 32 * 1.0
+    A_find = b_in_find + 9 + 32 * rho + 32 * hit
+    up_ms, up_n = prof["upsert"]
+    lk_ms, lk_n = prof["lookup"]
+    peak, peak_kind = load_peaks()
+    kernels = {
+        "upsert": {"launches": up_n, "ms_total": up_ms, "bytes_per_launch": A_up * P_up / max(1, up_n / args.steps),
+                   "algorithmic_bytes_per_kmer": A_up},
+        "lookup": {"launches": lk_n, "ms_total": lk_ms, "bytes_per_launch": A_find * P_find / max(1, lk_n / args.steps),
+                   "algorithmic_bytes_per_kmer": A_find},
+    }
+    for kv in kernels.values():
+        kv["achieved_gbs"] = kv["bytes_per_launch"] / (kv["ms_total"] / max(1, kv["launches"]) * 1e-3) / 1e9 if kv["ms_total"] else None
+    dom = max(kernels, key=lambda k_: kernels[k_]["ms_total"])
+    d = kernels[dom]
+
+    # End to end through the C interface with host buffers.
+    for _ in range(max(1, args.warmup // 2)):
+        step_e2e()
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        step_e2e()
+    barrier()
+    e2e_ms = max_over_ranks((time.perf_counter() - t0) * 1000) / args.steps
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": P * ws / (ms * 1e-3), "unit": "k-mers/s", "n_gpus": ws, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "u64", "data": "synthetic",
+            "config": {"workload": "config 1: <31,u64,22> n=10M; upsert(c+1, init 1) 333,333 x 150 bp; find 1M x 150 bp held-out",
+                       "upsert_positions": P_up, "find_positions": P_find, "keys": inserted, "capacity": st.capacity,
+                       "placed_pct": [round(st.primary_pct, 3), round(st.secondary_pct, 3), round(st.overflow_pct, 3)],
+                       "l2": "inputs larger than L2 (reads 250 MB + table 240 MB per step)", "parallelism": f"{ws} independent tables"},
+            "gpu_launches": launches,
+            "roofline": {"bound": "hbm", "kernel": dom, "achieved": d["achieved_gbs"], "peak": peak, "unit": "GB/s",
+                         "frac": (d["achieved_gbs"] / peak) if d["achieved_gbs"] else None, "traffic": None,
+                         "peak_source": peak_kind, "kernels": kernels,
+                         "model": "A = b_in + b_out + 32*rho + 32*r_slot + 32*w_slot bytes per k-mer; rho from the describer on 5000 reads"},
+            "e2e": {"value": P * ws / (e2e_ms * 1e-3), "unit": "k-mers/s", "ms_per_step": e2e_ms,
+                    "h2d_bytes_per_step": int(bi.off[-1] + bh.off[-1] + 16 * (bi.n + bh.n)),
+                    "d2h_bytes_per_step": int(P_find * 9)},
+            "clocks": clk,
+        }
+        cb = cpu_baseline_sample(ins, held, min(128, os.cpu_count() or 1))
+        line["cpu_baseline"] = cb
+        print(json.dumps(line))
+    T.close()
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def run_density(kache, b):
+    """Minimizer runs per k-mer position (rho): the share of positions whose minimizer hash differs from the previous
+    position's in the same sequence, from the describer."""
+    t = kache.Table(31, 0, 1000)
+    key, h, cs, fwd, valid = t.describe(b)
+    t.close()
+    pos = b.positions(31)
+    starts = np.zeros(len(h), bool)
+    o = np.concatenate([[0], np.cumsum(pos)[:-1]]).astype(np.int64)
+    starts[o[pos > 0]] = True
+    change = np.ones(len(h), bool)
+    change[1:] = h[1:] != h[:-1]
+    runs = (change | starts) & (valid == 1)
+    return float(runs.sum()) / max(1, int(valid.sum()))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    args = ap.parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_b200(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,89 @@
+/* Extensions of the B200 kache-hash library beyond the reference's C interface.
+ *
+ * These expose what the reference offers only through its C++ templates (other k and l, the template API's
+ * wrapping `v + x`, separate initial values; include/Streaming_Kmer_Hash_Table.hpp:624-745), its counter library
+ * (counter/Kmer_Set_Counter.hpp:23-76), and what a GPU caller needs on top: batches already resident in HBM,
+ * the CUDA stream to run on, and per-kernel timing. Tables made here are kache_table handles: every kache_* function
+ * of kache_capi.h works on them.
+ */
+#ifndef KACHE_B200_H
+#define KACHE_B200_H
+
+#include "kache_capi.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* An operation beyond the reference C interface's: v + x modulo 2^(8 * value_bytes), the template API's counting
+ * functor (test/check.cpp `inc`, counter/Kmer_Set_Counter.cpp:85). */
+#define KACHE_B200_ADD_WRAP 16u
+
+/* Creates a table of k-mers with l-minimizers: (k, l) one of (31, 22), (27, 16), (32, 20); value_bytes 0, 1, 2, 4,
+ * 8; sized as the reference's Streaming_Kmer_Hash_Table(expected_keys, workers, load_factor, pow2_capacity)
+ * (include/Streaming_Kmer_Hash_Table.hpp:624,771-796). */
+int kache_b200_new(uint32_t k, uint32_t l, uint32_t value_bytes, uint64_t expected_keys, double load_factor, uint32_t pow2_capacity, kache_table** out) KACHE_NOEXCEPT;
+
+/* Runs the table's work on the CUDA stream `stream` (a cudaStream_t; NULL for the table's own stream). */
+int kache_b200_set_stream(kache_table* t, void* stream) KACHE_NOEXCEPT;
+
+/* upsert with the initial value `init` for absent keys and f(v) = op(v, x) for present ones, op including
+ * KACHE_B200_ADD_WRAP (include/Streaming_Kmer_Hash_Table.hpp:672). In a set, an insert. */
+int kache_b200_upsert(kache_table* t, uint32_t user, const char* const* seqs, const size_t* lens, size_t n, uint32_t op, uint64_t x, uint64_t init, uint64_t* inserted) KACHE_NOEXCEPT;
+
+/* upsert_oriented with op one of KACHE_ASSIGN, KACHE_ADD, KACHE_OR, KACHE_MAX, KACHE_B200_ADD_WRAP
+ * (include/Streaming_Kmer_Hash_Table.hpp:682). */
+int kache_b200_upsert_oriented(kache_table* t, uint32_t user, const char* const* seqs, const size_t* lens, size_t n, uint32_t op, uint64_t x_fwd, uint64_t x_rev, uint64_t* inserted) KACHE_NOEXCEPT;
+
+/* update with op including KACHE_B200_ADD_WRAP (include/Streaming_Kmer_Hash_Table.hpp:698). */
+int kache_b200_update(kache_table* t, const char* const* seqs, const size_t* lens, size_t n, uint32_t op, uint64_t x, uint64_t* present) KACHE_NOEXCEPT;
+
+/* Batches resident in device memory: sequence i is d_bases[d_off[i], d_off[i + 1]), d_off holding n + 1 offsets.
+ * Outputs of the lookups are device pointers too, laid out as kache_lookup's. Results returned by value
+ * (inserted, present) are read back, so each call ends synchronised with its stream. */
+int kache_b200_upsert_dev(kache_table* t, uint32_t user, const uint8_t* d_bases, const uint64_t* d_off, uint64_t n, uint32_t op, uint64_t x, uint64_t init, uint64_t* inserted) KACHE_NOEXCEPT;
+int kache_b200_upsert_oriented_dev(kache_table* t, uint32_t user, const uint8_t* d_bases, const uint64_t* d_off, uint64_t n, uint32_t op, uint64_t x_fwd, uint64_t x_rev, uint64_t* inserted) KACHE_NOEXCEPT;
+int kache_b200_update_dev(kache_table* t, const uint8_t* d_bases, const uint64_t* d_off, uint64_t n, uint32_t op, uint64_t x, uint64_t* present) KACHE_NOEXCEPT;
+int kache_b200_lookup_dev(kache_table* t, const uint8_t* d_bases, const uint64_t* d_off, uint64_t n, uint8_t* d_found, void* d_values, uint8_t* d_fwd) KACHE_NOEXCEPT;
+int kache_b200_count_dev(kache_table* t, const uint8_t* d_bases, const uint64_t* d_off, uint64_t n, uint64_t* d_counts) KACHE_NOEXCEPT;
+
+/* The describer's output per position, laid out as kache_lookup's: canonical key, minimizer hash, checksum,
+ * orientation, whether the k characters are all ACGT. For checking the describer against the reference's. */
+int kache_b200_describe(kache_table* t, const char* const* seqs, const size_t* lens, size_t n, uint64_t* key, uint64_t* h, uint8_t* cs, uint8_t* fwd, uint8_t* valid) KACHE_NOEXCEPT;
+
+/* The histogram of values in [1, max] into h[0..max] (h[0] = 0) (counter/Kmer_Set_Counter.cpp:96-119). */
+int kache_b200_histogram(kache_table* t, uint64_t max, uint64_t* h) KACHE_NOEXCEPT;
+
+/* Empties the table: no keys, the capacity it was created with, every user's pending count at 0; registered users
+ * stay registered. */
+int kache_b200_clear(kache_table* t) KACHE_NOEXCEPT;
+
+/* Device time and launch count of the table's kernels of one kind since profiling was switched on, measured with
+ * CUDA events recorded around each launch on the table's stream. Kinds: 0 upsert, 1 update, 2 lookup, 3 per-sequence
+ * reductions, 4 resize, 5 everything else. */
+int kache_b200_profile(kache_table* t, int on) KACHE_NOEXCEPT;
+int kache_b200_profile_read(kache_table* t, uint32_t kind, double* ms, uint64_t* launches) KACHE_NOEXCEPT;
+
+/* Kernels this library has launched in this process, over all tables. */
+uint64_t kache_b200_kernel_launches(void) KACHE_NOEXCEPT;
+
+/* The counter library (counter/Kmer_Set_Counter.hpp:23-76): a set of 31-mers primed at count 0 and counted by
+ * present-only increments that wrap at 2^32. Paths name FASTA or FASTQ files, or pipes. */
+typedef struct kache_counter kache_counter;
+int kache_counter_new(uint32_t k, uint64_t n, uint32_t threads, double load_factor, kache_counter** out) KACHE_NOEXCEPT;
+void kache_counter_free(kache_counter* c) KACHE_NOEXCEPT;
+int kache_counter_prime(kache_counter* c, const char* path) KACHE_NOEXCEPT;
+int kache_counter_count(kache_counter* c, const char* path, uint64_t* found) KACHE_NOEXCEPT;
+int kache_counter_prime_batch(kache_counter* c, const char* const* seqs, const size_t* lens, size_t n) KACHE_NOEXCEPT;
+int kache_counter_count_batch(kache_counter* c, const char* const* seqs, const size_t* lens, size_t n, uint64_t* found) KACHE_NOEXCEPT;
+int kache_counter_histogram(kache_counter* c, uint64_t max, uint64_t* h) KACHE_NOEXCEPT;
+int kache_counter_count_of(kache_counter* c, const char* kmer, uint64_t* count) KACHE_NOEXCEPT;
+int kache_counter_size(kache_counter* c, uint64_t* n) KACHE_NOEXCEPT;
+/* The counter's table, for the kache_* queries (do not free it). */
+kache_table* kache_counter_table(kache_counter* c) KACHE_NOEXCEPT;
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

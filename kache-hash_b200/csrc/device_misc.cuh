@@ -1,0 +1,246 @@
+// The table-wide kernels: resize (rehash into a doubled table), overflow growth, iteration (for_each), reductions,
+// histograms, placement statistics, single-k-mer lookups, and the device-side batch preparation.
+#pragma once
+
+#include "device_table.cuh"
+#include "device_stream.cuh"
+
+namespace kache_b200
+{
+
+// Inserts one key with its value, known absent (every key of a table is distinct), into `T`. Returns INSERTED or
+// OV_FULL.
+template <bool set_>
+__device__ __forceinline__ uint32_t place_key(const Dev_Table& T, const uint64_t key, const uint64_t h, const unsigned long long val)
+{
+    Landing L{};
+    const uint32_t r = upsert_chain<set_>(T, key, h, checksum_of(key), L);
+    if(r == INSERTED)
+    {
+        if constexpr(!set_)
+            *L.val = val;
+        publish(L, !set_);
+        if(!L.cs)
+            atomicAdd(T.ov_count, 1ull);
+    }
+    return r;
+}
+
+// Resize (include/Streaming_Kmer_Hash_Table.hpp:1474-1681, out of place): every key of the old table, from its
+// buckets and its overflow table, goes into the new one; minimizer hashes are recomputed from the keys
+// (include/Streaming_Kmer_Hash_Table.hpp:1459-1470). A thread per old slot. Keys that find the new overflow table
+// full set their bit in `retry_out`; with `retry_in`, only those run.
+template <int k, int l, bool set_>
+__global__ void __launch_bounds__(256) rehash_kernel(const Dev_Table from, const Dev_Table to, const unsigned int* retry_in, unsigned int* retry_out, unsigned int* retried)
+{
+    const uint64_t main_slots = from.cap * B, total = main_slots + from.ov_mask + 1;
+    for(uint64_t s = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; s < total; s += uint64_t(gridDim.x) * blockDim.x)
+    {
+        if(retry_in && !((retry_in[s >> 5] >> (s & 31)) & 1))
+            continue;
+        unsigned long long key_st, val = 0;
+        if(s < main_slots)
+        {
+            if(from.cs[s] == 0)
+                continue;
+            key_st = from.slots[s * slot_words<set_>()];
+            if constexpr(!set_)
+                val = from.slots[s * 2 + 1];
+        }
+        else
+        {
+            const uint64_t i = s - main_slots;
+            key_st = from.ov[4 * i];
+            if(key_st == 0)
+                continue;
+            val = from.ov[4 * i + 1];
+        }
+        const uint64_t key = ~key_st;
+        if(place_key<set_>(to, key, minimizer_hash<k, l>(key), val) == OV_FULL)
+        {
+            atomicOr(retry_out + (s >> 5), 1u << (s & 31));
+            *retried = 1;
+        }
+    }
+}
+
+// Doubles the overflow table: re-inserts its keys into `to`'s overflow table, which has nothing else.
+static __global__ void __launch_bounds__(256) ov_move_kernel(const unsigned long long* from, const uint64_t from_slots, const Dev_Table to)
+{
+    for(uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < from_slots; i += uint64_t(gridDim.x) * blockDim.x)
+    {
+        const unsigned long long key_st = from[4 * i];
+        if(key_st == 0)
+            continue;
+        // The target has twice the slots, so a free one lies within its capacity.
+        uint64_t j = ov_hash(key_st) & to.ov_mask;
+        for(uint64_t t = 0; t <= to.ov_mask; ++t, j = (j + 1) & to.ov_mask)
+            if(atomicCAS(to.ov + 4 * j, 0ull, key_st) == 0ull)
+            {
+                to.ov[4 * j + 1] = from[4 * i + 1];
+                to.ov[4 * j + 2] = 1;
+                break;
+            }
+    }
+}
+
+// Collects the keys (as their 2-bit encodings) and values of buckets [b_b, b_e) and overflow slots [o_b, o_e), in
+// no particular order (include/Streaming_Kmer_Hash_Table.hpp:2705-2725): a warp claims its output range with one
+// atomic.
+template <bool set_>
+__global__ void __launch_bounds__(256) collect_kernel(const Dev_Table T, const uint64_t b_b, const uint64_t b_e, const uint64_t o_b, const uint64_t o_e,
+                                                      uint64_t* keys, uint64_t* vals, unsigned long long* count)
+{
+    const uint64_t n_main = (b_e - b_b) * B, total = n_main + (o_e - o_b);
+    const uint32_t lane = threadIdx.x & 31;
+    const uint64_t stride = uint64_t(gridDim.x) * blockDim.x;
+    for(uint64_t s0 = uint64_t(blockIdx.x) * blockDim.x; s0 < total; s0 += stride)
+    {
+        const uint64_t s = s0 + threadIdx.x;
+        bool have = false;
+        unsigned long long key_st = 0, val = 0;
+        if(s < n_main)
+        {
+            const uint64_t slot = b_b * B + s;
+            if(T.cs[slot])
+            {
+                have = true;
+                key_st = T.slots[slot * slot_words<set_>()];
+                if constexpr(!set_)
+                    val = T.slots[slot * 2 + 1];
+            }
+        }
+        else if(s < total)
+        {
+            const uint64_t i = o_b + (s - n_main);
+            key_st = T.ov[4 * i];
+            if(key_st)
+                have = true, val = T.ov[4 * i + 1];
+        }
+        const uint32_t m = __ballot_sync(0xFFFFFFFFu, have);
+        unsigned long long base = 0;
+        if(lane == 0 && m)
+            base = atomicAdd(count, static_cast<unsigned long long>(__popc(m)));
+        base = __shfl_sync(0xFFFFFFFFu, base, 0);
+        if(have)
+        {
+            const uint64_t o = base + __popc(m & ((1u << lane) - 1));
+            keys[o] = ~key_st;
+            if(vals)
+                vals[o] = val;
+        }
+    }
+}
+
+// Reductions of the C interface over all keys (capi/Kmer_Table.hpp:203-230): 0 keys with v & m nonzero (all keys
+// in a set), 1 popcount of v & m, 2 sum of v & m; and 3, the histogram of values in [1, max] (counter/
+// Kmer_Set_Counter.cpp:96-119), into `hist`.
+template <bool set_, typename V>
+__global__ void __launch_bounds__(256) reduce_kernel(const Dev_Table T, const uint32_t what, const uint64_t mask, unsigned long long* out, const uint64_t hmax, unsigned long long* hist)
+{
+    const uint64_t n_main = T.cap * B, total = n_main + T.ov_mask + 1;
+    unsigned long long acc = 0;
+    for(uint64_t s = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; s < total; s += uint64_t(gridDim.x) * blockDim.x)
+    {
+        bool have;
+        unsigned long long raw = 0;
+        if(s < n_main)
+        {
+            have = T.cs[s] != 0;
+            if constexpr(!set_)
+                if(have)
+                    raw = T.slots[s * 2 + 1];
+        }
+        else
+        {
+            const uint64_t i = s - n_main;
+            have = T.ov[4 * i] != 0;
+            if(have)
+                raw = T.ov[4 * i + 1];
+        }
+        if(!have)
+            continue;
+        const uint64_t v = static_cast<uint64_t>(static_cast<V>(raw));
+        if(what == 3)
+        {
+            if(v >= 1 && v <= hmax)
+                atomicAdd(hist + v, 1ull);
+            continue;
+        }
+        const uint64_t x = v & mask;
+        if(set_)
+            acc += 1;
+        else if(what == 0)
+            acc += x != 0;
+        else if(what == 1)
+            acc += __popcll(x);
+        else
+            acc += x;
+    }
+#pragma unroll
+    for(int o = 16; o > 0; o >>= 1)
+        acc += __shfl_xor_sync(0xFFFFFFFFu, acc, o);
+    if((threadIdx.x & 31) == 0 && acc)
+        atomicAdd(out, acc);
+}
+
+// Placement statistics (include/Streaming_Kmer_Hash_Table.hpp:1108-1120,2729-2752): keys in their primary bucket
+// and keys in another, from recomputed minimizer hashes.
+template <int k, int l, bool set_>
+__global__ void __launch_bounds__(256) distribution_kernel(const Dev_Table T, unsigned long long* prim_sec)
+{
+    const uint64_t n_main = T.cap * B;
+    unsigned long long p = 0, s2 = 0;
+    for(uint64_t s = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; s < n_main; s += uint64_t(gridDim.x) * blockDim.x)
+    {
+        if(!T.cs[s])
+            continue;
+        const uint64_t key = ~T.slots[s * slot_words<set_>()];
+        if(bucket_of(minimizer_hash<k, l>(key), T.cap) == s / B)
+            p++;
+        else
+            s2++;
+    }
+#pragma unroll
+    for(int o = 16; o > 0; o >>= 1)
+        p += __shfl_xor_sync(0xFFFFFFFFu, p, o), s2 += __shfl_xor_sync(0xFFFFFFFFu, s2, o);
+    if((threadIdx.x & 31) == 0)
+        atomicAdd(prim_sec, p), atomicAdd(prim_sec + 1, s2);
+}
+
+// Single k-mer lookups (include/Streaming_Kmer_Hash_Table.hpp:2608-2645) of canonical keys: out[2i] = found,
+// out[2i+1] = value.
+template <int k, int l, bool set_, typename V>
+__global__ void get_kernel(const Dev_Table T, const uint64_t* keys, const uint64_t n, unsigned long long* out)
+{
+    const uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if(i >= n)
+        return;
+    const uint64_t key = keys[i];
+    const unsigned long long* v = find_chain<set_, false>(T, key, minimizer_hash<k, l>(key), checksum_of(key));
+    out[2 * i] = v != nullptr;
+    out[2 * i + 1] = (v && !set_) ? static_cast<unsigned long long>(read_val<V>(v)) : 0ull;
+}
+
+// Device-side batch preparation, for batches already in HBM: per sequence, its positions and segments.
+static __global__ void batch_counts_kernel(const uint64_t* off, const uint64_t n, const int k, uint64_t* npos, uint64_t* nseg)
+{
+    const uint64_t q = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if(q >= n)
+        return;
+    const uint64_t len = off[q + 1] - off[q];
+    const uint64_t p = len >= uint64_t(k) ? len - k + 1 : 0;
+    npos[q] = p;
+    nseg[q] = (p + seg_positions - 1) / seg_positions;
+}
+
+static __global__ void batch_segs_kernel(const uint64_t* seg_off, const uint64_t n, uint64_t* segs)
+{
+    const uint64_t q = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if(q >= n)
+        return;
+    for(uint64_t g = seg_off[q], s = 0; g < seg_off[q + 1]; ++g, ++s)
+        segs[g] = (q << 24) | s;
+}
+
+}

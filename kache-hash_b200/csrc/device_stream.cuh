@@ -1,0 +1,349 @@
+// The warp describer and the streaming kernel: one warp describes a segment of a sequence, 32 k-mer positions per
+// row, and hands each row's k-mers to a visitor (upsert, update, lookup, count, ...), one k-mer per lane.
+//
+// What it computes per position is the reference describers' description (include/Kmer_Batch.hpp:191-250,
+// include/Kmer_Lanes.hpp:164-244): the canonical key, its orientation, its checksum and its l-minimizer hash. How:
+//   - each row of 32 bases is loaded coalesced (lane j reads base j), turned into 2-bit codes and an ACGT bit, and
+//     packed with three ballots into a forward word W (first base most significant) and a complemented word R
+//     (first base least significant), once per row rather than once per k-mer;
+//   - lane j's k-mer is a 2k-bit funnel window of (W_r, W_r+1) and its reverse complement one of (R_r, R_r+1);
+//   - l-mer hashes of a row go to a per-warp ring in shared memory, and a k-mer's minimizer hash is the least of
+//     the w = k - l + 1 hashes from its own position on;
+//   - non-ACGT characters split sequences (DNA_Utility.hpp:199-224): a window with one is not a k-mer.
+// Sequences are cut into segments of up to `seg_positions` positions; each segment re-reads the k - 1 bases it
+// shares with the next, so segments, like the reference's lanes (include/Streaming_Kmer_Hash_Table.hpp:1751-1781),
+// need no state from one another.
+#pragma once
+
+#include "device_table.cuh"
+
+namespace kache_b200
+{
+
+// A batch on the device: sequence q is bases[off[q], off[q+1]); segs lists (q << 24 | s) for the s'th segment of
+// each sequence of at least k bases; pos_off[q] counts the positions of the sequences before q.
+struct Dev_Batch
+{
+    const uint8_t* bases;
+    const uint64_t* off;
+    const uint64_t* segs;
+    const uint64_t* pos_off;
+    uint64_t n;
+    uint64_t nsegs;
+};
+
+constexpr int stream_warps = 8;
+
+// One row of 32 bases, packed.
+struct Row
+{
+    uint64_t W, R;
+    uint32_t valid;
+};
+
+__device__ __forceinline__ Row load_row(const uint8_t* seq, const uint64_t len, const uint64_t p, const uint32_t lane)
+{
+    const uint64_t pos = p + lane;
+    const uint32_t ch = pos < len ? seq[pos] : 0u;
+    const uint32_t x = ch | 0x20u;
+    const bool ok = (x == 'a') | (x == 'c') | (x == 'g') | (x == 't');
+    const uint32_t code = ((ch >> 2) ^ (ch >> 1)) & 3u;
+    const uint32_t lo = __ballot_sync(0xFFFFFFFFu, code & 1u);
+    const uint32_t hi = __ballot_sync(0xFFFFFFFFu, code >> 1);
+    Row r;
+    r.valid = __ballot_sync(0xFFFFFFFFu, ok);
+    const uint64_t z = spread32(lo) | (spread32(hi) << 1);   // Base j at bits 2j, 2j+1.
+    uint64_t t = __brevll(z);
+    r.W = ((t >> 1) & 0x5555555555555555ull) | ((t & 0x5555555555555555ull) << 1);  // Base 0 at bits 63..62.
+    r.R = ~z;   // Complemented bases, base j at bits 2j.
+    return r;
+}
+
+// The forward and reverse-complement n-mers (n <= 32) starting at base j of row a, spilling into row b.
+template <int n>
+__device__ __forceinline__ void window(const Row& a, const Row& b, const uint32_t j, uint64_t& f, uint64_t& r)
+{
+    const uint32_t s = 2 * j;
+    const uint64_t top = (a.W << s) | ((b.W >> (63 - s)) >> 1);
+    f = top >> (64 - 2 * n);
+    const uint64_t low = (a.R >> s) | ((b.R << (63 - s)) << 1);
+    r = low & kmer_mask(n);
+}
+
+// A k-mer as the visitors get it.
+struct Kmer_Desc
+{
+    uint64_t key, h;
+    uint64_t q, pos;    // Sequence and position in it.
+    uint8_t c;
+    bool fwd;           // Occurs as its canonical form.
+    bool valid;         // All k characters are ACGT.
+    bool in;            // The position exists (is in the segment).
+};
+
+template <int k, int l, typename Visitor>
+__global__ void __launch_bounds__(32 * stream_warps) stream_kernel(const Dev_Batch batch, const uint64_t seg_b, const uint64_t seg_e, Visitor vis)
+{
+    constexpr int w = k - l + 1;
+    static_assert(k <= 32 && l <= k && w <= 32, "k-mers in a machine word");
+    __shared__ uint64_t ring_all[stream_warps][64];
+    const uint32_t lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    uint64_t* ring = ring_all[wid];
+    vis.begin();
+
+    const uint64_t warps = uint64_t(gridDim.x) * stream_warps;
+    for(uint64_t g = seg_b + uint64_t(blockIdx.x) * stream_warps + wid; g < seg_e; g += warps)
+    {
+        const uint64_t packed = batch.segs[g];
+        const uint64_t q = packed >> 24, s = packed & 0xFFFFFF;
+        const uint64_t b0 = batch.off[q], len = batch.off[q + 1] - b0;
+        const uint8_t* seq = batch.bases + b0;
+        const uint64_t npos = len - k + 1;
+        const uint64_t p0 = s * seg_positions;
+        const uint64_t p1 = min(npos, p0 + seg_positions);
+        const uint32_t rows = static_cast<uint32_t>((p1 - p0 + 31) / 32);
+
+        Row r0 = load_row(seq, len, p0, lane);
+        Row r1 = load_row(seq, len, p0 + 32, lane);
+        {
+            uint64_t f, rc;
+            window<l>(r0, r1, lane, f, rc);
+            ring[lane] = wang_u64(f < rc ? f : rc);
+        }
+
+        vis.begin_segment(q);
+        for(uint32_t r = 0; r < rows; ++r)
+        {
+            const Row r2 = load_row(seq, len, p0 + 32 * (r + 2), lane);
+            {
+                uint64_t f, rc;
+                window<l>(r1, r2, lane, f, rc);
+                ring[((r + 1) & 1) * 32 + lane] = wang_u64(f < rc ? f : rc);
+            }
+            __syncwarp();
+
+            Kmer_Desc d;
+            uint64_t f, rc;
+            window<k>(r0, r1, lane, f, rc);
+            const uint64_t vbits = ((uint64_t(r1.valid) << 32) | r0.valid) >> lane;
+            const uint64_t km = (k == 32 ? 0xFFFFFFFFull : (1ull << k) - 1);
+            d.pos = p0 + 32 * r + lane;
+            d.q = q;
+            d.in = d.pos < p1;
+            d.valid = d.in && (vbits & km) == km;
+            d.key = f < rc ? f : rc;
+            d.fwd = f <= rc;
+            d.c = checksum_of(d.key);
+            uint64_t h = ~0ull;
+            const uint32_t base = (r & 1) * 32 + lane;
+#pragma unroll
+            for(int x = 0; x < w; ++x)
+            {
+                const uint64_t v = ring[(base + x) & 63];
+                h = v < h ? v : h;
+            }
+            d.h = h;
+
+            vis.visit(d, lane);
+            __syncwarp();
+            r0 = r1, r1 = r2;
+        }
+        vis.end_segment(q, lane);
+    }
+    vis.end(lane);
+}
+
+// ---- Visitors -------------------------------------------------------------------------------------------------
+
+// Per-warp counter flush: one atomic per warp at the end of the kernel.
+__device__ __forceinline__ void warp_flush(unsigned long long* ctr, const unsigned long long c, const uint32_t lane)
+{
+    if(lane == 0 && c)
+        atomicAdd(ctr, c);
+}
+
+// Upsert / insert / upsert_oriented (include/Streaming_Kmer_Hash_Table.hpp:2219-2514): returns the keys inserted;
+// k-mers that found the overflow table full set their bit in `retry_out` and change nothing. In retry mode, only
+// the positions whose bit is set in `retry_in` run.
+template <bool set_, typename V, typename Fn>
+struct Upsert_Visitor
+{
+    Dev_Table T;
+    Fn fn;
+    const uint64_t* pos_off;
+    unsigned long long* inserted;
+    unsigned int* retry_out;
+    const unsigned int* retry_in;
+    unsigned int* retried;      // Set to 1 if any bit of retry_out was set.
+    unsigned long long ins;
+
+    __device__ __forceinline__ void begin() { ins = 0; }
+    __device__ __forceinline__ void begin_segment(uint64_t) {}
+    __device__ __forceinline__ void end_segment(uint64_t, uint32_t) {}
+
+    __device__ __forceinline__ void visit(const Kmer_Desc& d, const uint32_t lane)
+    {
+        bool active = d.valid;
+        if(retry_in && active)
+        {
+            const uint64_t gpos = pos_off[d.q] + d.pos;
+            active = (retry_in[gpos >> 5] >> (gpos & 31)) & 1;
+        }
+
+        Landing L{};
+        uint32_t r = NONE;
+        if(active)
+            r = upsert_chain<set_>(T, d.key, d.h, d.c, L);
+        if(r == INSERTED)
+        {
+            if constexpr(!set_)
+                write_val<V>(L.val, fn.initial(d.fwd));
+            publish(L, !set_);
+        }
+        else if(r == OV_FULL)
+        {
+            const uint64_t gpos = pos_off[d.q] + d.pos;
+            atomicOr(retry_out + (gpos >> 5), 1u << (gpos & 31));
+            *retried = 1;
+        }
+        ins += __popc(__ballot_sync(0xFFFFFFFFu, r == INSERTED));
+        __syncwarp();
+
+        if constexpr(!set_)
+            if((r == FOUND || r == FOUND_PENDING) && !fn.is_noop())
+            {
+                if(r == FOUND_PENDING && !await_published(L))
+                    atomicOr(T.err, ERR_WAIT);
+                fn.apply(L.val, d.fwd);
+            }
+        if(r == INSERTED && !L.cs)
+            atomicAdd(T.ov_count, 1ull);
+    }
+
+    __device__ __forceinline__ void end(const uint32_t lane) { warp_flush(inserted, ins, lane); }
+};
+
+// Present-only update (include/Streaming_Kmer_Hash_Table.hpp:2650-2691): returns the k-mers present, repeats counted.
+template <typename V, typename Fn>
+struct Update_Visitor
+{
+    Dev_Table T;
+    Fn fn;
+    unsigned long long* present;
+    unsigned long long cnt;
+
+    __device__ __forceinline__ void begin() { cnt = 0; }
+    __device__ __forceinline__ void begin_segment(uint64_t) {}
+    __device__ __forceinline__ void end_segment(uint64_t, uint32_t) {}
+
+    __device__ __forceinline__ void visit(const Kmer_Desc& d, const uint32_t)
+    {
+        unsigned long long* v = nullptr;
+        if(d.valid)
+            v = find_chain<false, true>(T, d.key, d.h, d.c);
+        if(v)
+            fn.apply(v, d.fwd);
+        cnt += __popc(__ballot_sync(0xFFFFFFFFu, v != nullptr));
+    }
+
+    __device__ __forceinline__ void end(const uint32_t lane) { warp_flush(present, cnt, lane); }
+};
+
+// Per-position lookup (capi/Kmer_Table.hpp:163-190): found (0 absent, 1 present, 2 not a k-mer), value, orientation
+// at pos_off[q] + i.
+template <bool set_, typename V>
+struct Lookup_Visitor
+{
+    Dev_Table T;
+    const uint64_t* pos_off;
+    uint8_t* found;
+    V* values;
+    uint8_t* fwd;
+
+    __device__ __forceinline__ void begin() {}
+    __device__ __forceinline__ void begin_segment(uint64_t) {}
+    __device__ __forceinline__ void end_segment(uint64_t, uint32_t) {}
+    __device__ __forceinline__ void end(uint32_t) {}
+
+    __device__ __forceinline__ void visit(const Kmer_Desc& d, const uint32_t)
+    {
+        const unsigned long long* v = nullptr;
+        if(d.valid)
+            v = find_chain<set_, false>(T, d.key, d.h, d.c);
+        if(!d.in)
+            return;
+        const uint64_t o = pos_off[d.q] + d.pos;
+        found[o] = d.valid ? (v ? 1 : 0) : 2;
+        if constexpr(!set_)
+            if(values)
+                values[o] = v ? read_val<V>(v) : V(0);
+        if(fwd)
+            fwd[o] = d.valid && d.fwd;
+    }
+};
+
+// Per-sequence reductions over lookups (capi/Kmer_Table.hpp:134-161): 0 count, 1 masked count, 2 sum. A segment
+// belongs to one sequence, so each warp adds its segment's total once.
+template <bool set_, typename V, int mode_>
+struct Seq_Reduce_Visitor
+{
+    Dev_Table T;
+    unsigned long long* out;
+    V m_fwd, m_rev;
+    unsigned long long acc;
+    unsigned long long total;
+
+    __device__ __forceinline__ void begin() { total = 0; }
+    __device__ __forceinline__ void begin_segment(uint64_t) { acc = 0; }
+    __device__ __forceinline__ void visit(const Kmer_Desc& d, const uint32_t)
+    {
+        if(!d.valid)
+            return;
+        const unsigned long long* v = find_chain<set_, false>(T, d.key, d.h, d.c);
+        if(!v)
+            return;
+        if constexpr(mode_ == 0)
+            acc += 1;
+        else if constexpr(mode_ == 1)
+            acc += (read_val<V>(v) & (d.fwd ? m_fwd : m_rev)) != 0;
+        else
+            acc += static_cast<unsigned long long>(read_val<V>(v));
+    }
+    __device__ __forceinline__ void end_segment(const uint64_t q, const uint32_t lane)
+    {
+        unsigned long long a = acc;
+#pragma unroll
+        for(int o = 16; o > 0; o >>= 1)
+            a += __shfl_xor_sync(0xFFFFFFFFu, a, o);
+        if(lane == 0 && a)
+            atomicAdd(out + q, a);
+        total += a;
+    }
+    __device__ __forceinline__ void end(uint32_t) {}
+};
+
+// The descriptions themselves, for checking the describer.
+struct Describe_Visitor
+{
+    const uint64_t* pos_off;
+    uint64_t* key;
+    uint64_t* h;
+    uint8_t* cs;
+    uint8_t* fwd;
+    uint8_t* valid;
+
+    __device__ __forceinline__ void begin() {}
+    __device__ __forceinline__ void begin_segment(uint64_t) {}
+    __device__ __forceinline__ void end_segment(uint64_t, uint32_t) {}
+    __device__ __forceinline__ void end(uint32_t) {}
+    __device__ __forceinline__ void visit(const Kmer_Desc& d, const uint32_t)
+    {
+        if(!d.in)
+            return;
+        const uint64_t o = pos_off[d.q] + d.pos;
+        key[o] = d.valid ? d.key : 0, h[o] = d.valid ? d.h : 0, cs[o] = d.valid ? d.c : 0;
+        fwd[o] = d.valid && d.fwd, valid[o] = d.valid;
+    }
+};
+
+}

@@ -1,0 +1,948 @@
+// Host side of the B200 table: device memory, batch staging, the sizing and resize schedule, and the launches.
+//
+// One Engine<k, l, V> owns one table in HBM. Its operations are those of the reference's
+// Streaming_Kmer_Hash_Table<k, true, V, l> (include/Streaming_Kmer_Hash_Table.hpp:624-745), with the value
+// functions as device functors. The capacity follows the reference exactly: cap_for at construction, then one
+// doubling wherever the reference's per-user flush schedule would resize (:2244-2286, :1447-1455, :1679-1680);
+// that schedule depends only on the per-call counts of inserted keys, which the kernels return exactly. The GPU
+// table itself resizes between launches: a call's batch is cut into chunks sized so the table stays below full,
+// and after each chunk the table is rebuilt at the capacity the schedule has reached.
+#pragma once
+
+#include "device_misc.cuh"
+#include "kache_capi.h"
+
+#include <cub/device/device_scan.cuh>
+
+#include <algorithm>
+#include <atomic>
+#include <cmath>
+#include <cstring>
+#include <mutex>
+#include <new>
+#include <stdexcept>
+#include <string>
+#include <thread>
+#include <type_traits>
+#include <vector>
+
+// The object behind the C interface's opaque handle: a table of one (k, l, value width), behind virtual calls.
+struct kache_table
+{
+    const uint32_t kmer_k, kmer_l, value_bytes;   // k, l and the values' width (0 in a set).
+    std::mutex reg;                     // Serialises registrations.
+    std::atomic<uint32_t> user_c{0};    // Registered users.
+    mutable std::mutex work;            // Serialises the table's GPU work.
+
+    kache_table(uint32_t k, uint32_t l, uint32_t vb): kmer_k(k), kmer_l(l), value_bytes(vb) {}
+    virtual ~kache_table() = default;
+
+    virtual void set_stream(cudaStream_t s) = 0;
+    virtual uint64_t upsert(uint32_t user, const char* const* seqs, const size_t* lens, size_t n, uint32_t op, uint64_t x, uint64_t init) = 0;
+    virtual uint64_t upsert_oriented(uint32_t user, const char* const* seqs, const size_t* lens, size_t n, uint32_t op, uint64_t xf, uint64_t xr) = 0;
+    virtual uint64_t update(const char* const* seqs, const size_t* lens, size_t n, uint32_t op, uint64_t x) = 0;
+    virtual void lookup(const char* const* seqs, const size_t* lens, size_t n, uint8_t* found, void* values, uint8_t* fwd) = 0;
+    virtual void seq_reduce(const char* const* seqs, const size_t* lens, size_t n, int mode, uint64_t m_fwd, uint64_t m_rev, uint64_t* out) = 0;
+    virtual void describe(const char* const* seqs, const size_t* lens, size_t n, uint64_t* key, uint64_t* h, uint8_t* cs, uint8_t* fwd, uint8_t* valid) = 0;
+    virtual uint64_t upsert_dev(uint32_t user, const uint8_t* b, const uint64_t* off, uint64_t n, uint32_t op, uint64_t x, uint64_t init) = 0;
+    virtual uint64_t upsert_oriented_dev(uint32_t user, const uint8_t* b, const uint64_t* off, uint64_t n, uint32_t op, uint64_t xf, uint64_t xr) = 0;
+    virtual uint64_t update_dev(const uint8_t* b, const uint64_t* off, uint64_t n, uint32_t op, uint64_t x) = 0;
+    virtual void lookup_dev(const uint8_t* b, const uint64_t* off, uint64_t n, uint8_t* found, void* values, uint8_t* fwd) = 0;
+    virtual void count_dev(const uint8_t* b, const uint64_t* off, uint64_t n, uint64_t* counts) = 0;
+    virtual bool get(const char* kmer, uint64_t& value) = 0;
+    virtual uint64_t size() const = 0;
+    virtual uint64_t capacity() const = 0;
+    virtual uint64_t reduce(uint32_t what, uint64_t mask) = 0;
+    virtual void for_each(uint32_t shards, uint32_t shard, kache_keys_fn f, void* ctx) = 0;
+    virtual void histogram(uint64_t max, uint64_t* h) = 0;
+    virtual void get_stats(kache_stats& out) = 0;
+    virtual void clear() = 0;
+    virtual void profile(bool on) = 0;
+    virtual void profile_read(uint32_t kind, double& ms, uint64_t& launches) = 0;
+};
+
+namespace kache_b200
+{
+
+// A CUDA failure: the C interface maps it to KACHE_EINTERNAL; failed allocations throw std::bad_alloc instead.
+struct Cuda_Error : std::runtime_error
+{
+    using std::runtime_error::runtime_error;
+};
+
+inline void check(const cudaError_t e, const char* what)
+{
+    if(e == cudaSuccess)
+        return;
+    if(e == cudaErrorMemoryAllocation)
+    {
+        (void)cudaGetLastError();
+        throw std::bad_alloc();
+    }
+    throw Cuda_Error(std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+std::atomic<uint64_t>& launches();
+
+// ---- Sizing, as the reference's (include/Streaming_Kmer_Hash_Table.hpp:383, 800-804, 1004-1011) ----------------
+
+inline uint64_t ceil_pow2(uint64_t x)
+{
+    uint64_t p = 1;
+    while(p < x)
+        p <<= 1;
+    return p;
+}
+
+inline uint64_t cap_for(const uint64_t max_sz, const double lf, const bool pow2)
+{
+    uint64_t cap = std::max<uint64_t>(1, static_cast<uint64_t>(std::ceil(static_cast<double>(max_sz) / lf / B)));
+    while(static_cast<uint64_t>(static_cast<double>(cap * B) * lf) <= max_sz)
+        cap++;
+    return pow2 ? ceil_pow2(cap) : cap;
+}
+
+inline bool fits(const uint64_t max_sz, const double lf, const bool pow2)
+{
+    return static_cast<double>(max_sz) / lf / B <= static_cast<double>(max_buckets) && cap_for(max_sz, lf, pow2) <= max_buckets;
+}
+
+inline uint64_t step_for(const uint64_t th) { return std::clamp<uint64_t>(th / (8 * 128), 1, 16384); }
+
+// ---- Memory ----------------------------------------------------------------------------------------------------
+
+struct Dev_Buf
+{
+    void* p = nullptr;
+    size_t bytes = 0;
+
+    Dev_Buf() = default;
+    Dev_Buf(const Dev_Buf&) = delete;
+    Dev_Buf& operator=(const Dev_Buf&) = delete;
+    ~Dev_Buf() { release(); }
+
+    void release()
+    {
+        if(p)
+            cudaFree(p);
+        p = nullptr, bytes = 0;
+    }
+
+    // Grows to at least n bytes; the contents are lost on growth.
+    void ensure(const size_t n)
+    {
+        if(n <= bytes)
+            return;
+        release();
+        check(cudaMalloc(&p, std::max<size_t>(n, 256)), "cudaMalloc");
+        bytes = std::max<size_t>(n, 256);
+    }
+
+    template <typename T> T* as() const { return static_cast<T*>(p); }
+};
+
+struct Pinned_Buf
+{
+    void* p = nullptr;
+    size_t bytes = 0;
+
+    Pinned_Buf() = default;
+    Pinned_Buf(const Pinned_Buf&) = delete;
+    Pinned_Buf& operator=(const Pinned_Buf&) = delete;
+    ~Pinned_Buf() { release(); }
+
+    void release()
+    {
+        if(p)
+            cudaDeviceSynchronize(), cudaFreeHost(p);   // No copy may still read or write it.
+        p = nullptr, bytes = 0;
+    }
+
+    void ensure(const size_t n)
+    {
+        if(n <= bytes)
+            return;
+        release();
+        const size_t m = std::max<size_t>(n + n / 4, 1 << 20);
+        check(cudaHostAlloc(&p, m, cudaHostAllocDefault), "cudaHostAlloc");
+        bytes = m;
+    }
+
+    template <typename T> T* as(size_t byte_off = 0) const { return reinterpret_cast<T*>(static_cast<char*>(p) + byte_off); }
+};
+
+// Copies on up to `t_c` threads; small copies stay on this one.
+inline void parallel_for(const size_t n, const size_t min_per_thread, const auto& f)
+{
+    const size_t hw = std::max(1u, std::thread::hardware_concurrency());
+    const size_t t_c = std::min<size_t>(std::min<size_t>(hw, 32), std::max<size_t>(1, n / std::max<size_t>(1, min_per_thread)));
+    if(t_c <= 1)
+    {
+        f(size_t(0), n);
+        return;
+    }
+    std::vector<std::thread> W;
+    for(size_t t = 0; t < t_c; ++t)
+        W.emplace_back([&, t](){ f(n * t / t_c, n * (t + 1) / t_c); });
+    for(auto& w : W)
+        w.join();
+}
+
+inline bool host_acgt(const char c)
+{
+    const char x = static_cast<char>(c | 0x20);
+    return x == 'a' || x == 'c' || x == 'g' || x == 't';
+}
+
+// ---- The engine --------------------------------------------------------------------------------------------------
+
+enum Kind : uint32_t { K_UPSERT = 0, K_UPDATE = 1, K_LOOKUP = 2, K_REDUCE = 3, K_RESIZE = 4, K_OTHER = 5, K_KINDS = 6 };
+
+template <int k, int l, typename V>
+class Engine final : public kache_table
+{
+    static constexpr bool set_ = std::is_void_v<V>;
+    typedef typename Val_Of<V>::type VT;    // The values' type; a placeholder in a set.
+    static constexpr size_t slot_bytes = set_ ? 8 : 16;
+
+    cudaStream_t own_ = nullptr, stream_ = nullptr;
+    int sm_count_ = 148;
+
+    // The table.
+    Dev_Buf cs_, spill_, slots_, ov_, ctr_;
+    Dev_Table T_{};
+    uint64_t ov_slots_ = 0;
+
+    // The reference's sizing state (include/Streaming_Kmer_Hash_Table.hpp:81-86, 224-229).
+    const double lf_;
+    const uint64_t cap0_;
+    uint64_t cap_, resize_th_, step_, approx_sz_ = 0, size_ = 0;
+    uint64_t pending_[KACHE_MAX_USERS] = {};
+
+    // Batches.
+    Pinned_Buf pin_, pin_ctr_;
+    Dev_Buf dbatch_, dout_, dretry_a_, dretry_b_, dscan_, dtmp_;
+
+    // Profiling.
+    bool prof_ = false;
+    struct Ev { cudaEvent_t a, b; uint32_t kind; };
+    std::vector<Ev> ev_;
+    double prof_ms_[K_KINDS] = {};
+    uint64_t prof_n_[K_KINDS] = {};
+
+    // Device counters: [0] inserted/present, [1] overflow keys, [2] retry flag + error word, [3..4] scratch.
+    unsigned long long* ctr() const { return ctr_.as<unsigned long long>(); }
+
+    struct Batch_Info
+    {
+        Dev_Batch b{};
+        uint64_t total_pos = 0;
+    };
+
+    int grid_for(const uint64_t warps_needed, const int warps_per_block) const
+    {
+        const uint64_t blocks = (warps_needed + warps_per_block - 1) / warps_per_block;
+        return static_cast<int>(std::max<uint64_t>(1, std::min<uint64_t>(blocks, uint64_t(sm_count_) * 16)));
+    }
+
+    template <typename F> void launch(const uint32_t kind, const F& f)
+    {
+        Ev e{};
+        if(prof_)
+        {
+            check(cudaEventCreate(&e.a), "event"), check(cudaEventCreate(&e.b), "event");
+            e.kind = kind;
+            check(cudaEventRecord(e.a, stream_), "record");
+        }
+        f();
+        check(cudaGetLastError(), "kernel launch");
+        launches()++;
+        if(prof_)
+        {
+            check(cudaEventRecord(e.b, stream_), "record");
+            ev_.push_back(e);
+        }
+    }
+
+    void sync() { check(cudaStreamSynchronize(stream_), "cudaStreamSynchronize"); }
+
+    // Reads the device counters [0, n).
+    const unsigned long long* read_ctr(const int n)
+    {
+        check(cudaMemcpyAsync(pin_ctr_.p, ctr(), n * sizeof(unsigned long long), cudaMemcpyDeviceToHost, stream_), "D2H counters");
+        sync();
+        const auto* c = pin_ctr_.as<unsigned long long>();
+        if(c[2] >> 32)
+            throw Cuda_Error("a bounded device wait ran out");
+        return c;
+    }
+
+    void alloc_table(Dev_Buf& cs, Dev_Buf& spill, Dev_Buf& slots, const uint64_t cap)
+    {
+        cs.ensure(cap * B), spill.ensure(cap * 32), slots.ensure(cap * B * slot_bytes);
+        check(cudaMemsetAsync(cs.p, 0, cap * B, stream_), "memset");
+        check(cudaMemsetAsync(spill.p, 0, cap * 32, stream_), "memset");
+        check(cudaMemsetAsync(slots.p, 0, cap * B * slot_bytes, stream_), "memset");
+    }
+
+    // Overflow capacity for n keys at load 0.8, a power of 2 (include/Concurrent_Hash_Table.hpp:157-172).
+    static uint64_t ov_slots_for(const uint64_t n) { return ceil_pow2(static_cast<uint64_t>(std::ceil(static_cast<double>(n) / 0.8))); }
+
+    void set_ov(Dev_Table& T, Dev_Buf& ov, const uint64_t slots)
+    {
+        ov.ensure(slots * 32);
+        check(cudaMemsetAsync(ov.p, 0, slots * 32, stream_), "memset");
+        T.ov = ov.as<unsigned long long>();
+        T.ov_mask = slots - 1;
+        T.ov_probe = static_cast<uint32_t>(std::min<uint64_t>(slots, 4096));
+    }
+
+    void bind(Dev_Table& T, Dev_Buf& cs, Dev_Buf& spill, Dev_Buf& slots, const uint64_t cap)
+    {
+        T.cs = cs.as<uint8_t>(), T.spill = spill.as<uint32_t>(), T.slots = slots.as<unsigned long long>(), T.cap = cap;
+        T.ov_count = ctr() + 1;
+        T.err = reinterpret_cast<unsigned int*>(ctr() + 2) + 1;
+    }
+
+    // Doubles the overflow table.
+    void grow_overflow()
+    {
+        Dev_Buf nov;
+        Dev_Table T2 = T_;
+        const uint64_t old = ov_slots_;
+        set_ov(T2, nov, old * 2);
+        launch(K_OTHER, [&](){ ov_move_kernel<<<grid_for(old / 32 + 1, 8), 256, 0, stream_>>>(T_.ov, old, T2); });
+        std::swap(ov_.p, nov.p), std::swap(ov_.bytes, nov.bytes);
+        T_ = T2, T_.ov = ov_.as<unsigned long long>();
+        ov_slots_ = old * 2;
+        sync();
+    }
+
+    // Rebuilds the table at `new_cap` buckets (include/Streaming_Kmer_Hash_Table.hpp:1474-1681, out of place).
+    void resize(const uint64_t new_cap)
+    {
+        if(new_cap > max_buckets)
+            throw std::runtime_error("the table would exceed the most buckets supported");
+        Dev_Buf cs, spill, slots, ov;
+        alloc_table(cs, spill, slots, new_cap);
+        Dev_Table T2{};
+        bind(T2, cs, spill, slots, new_cap);
+        const uint64_t ov_keys = read_ctr(2)[1];
+        uint64_t ov_slots = ov_slots_for(std::max<uint64_t>({1024, new_cap, static_cast<uint64_t>(ov_keys * 1.5)}));
+        set_ov(T2, ov, ov_slots);
+        // The keys move, so the overflow count starts over.
+        check(cudaMemsetAsync(ctr() + 1, 0, sizeof(unsigned long long), stream_), "memset");
+
+        const uint64_t total = cap_ * B + ov_slots_;
+        dretry_a_.ensure(total / 8 + 8), dretry_b_.ensure(total / 8 + 8);
+        check(cudaMemsetAsync(dretry_a_.p, 0, total / 8 + 8, stream_), "memset");
+        unsigned int* retried = reinterpret_cast<unsigned int*>(ctr() + 2);
+        check(cudaMemsetAsync(retried, 0, 4, stream_), "memset");
+        launch(K_RESIZE, [&](){ rehash_kernel<k, l, set_><<<grid_for(total / 32 + 1, 8), 256, 0, stream_>>>(T_, T2, nullptr, dretry_a_.as<unsigned int>(), retried); });
+        while(static_cast<uint32_t>(read_ctr(3)[2]))
+        {
+            // The new overflow table filled up: double it, then retry the keys that found it full.
+            Dev_Buf nov;
+            Dev_Table T3 = T2;
+            set_ov(T3, nov, ov_slots * 2);
+            check(cudaMemsetAsync(ctr() + 1, 0, sizeof(unsigned long long), stream_), "memset");
+            launch(K_RESIZE, [&](){ ov_move_kernel<<<grid_for(ov_slots / 32 + 1, 8), 256, 0, stream_>>>(T2.ov, ov_slots, T3); });
+            const uint64_t moved = read_ctr(2)[1];
+            (void)moved;
+            std::swap(ov.p, nov.p), std::swap(ov.bytes, nov.bytes);
+            T2 = T3, T2.ov = ov.as<unsigned long long>();
+            ov_slots *= 2;
+            // ov_move_kernel does not count: recount by the slots it filled.
+            recount_overflow(T2, ov_slots);
+            check(cudaMemsetAsync(dretry_b_.p, 0, total / 8 + 8, stream_), "memset");
+            check(cudaMemsetAsync(retried, 0, 4, stream_), "memset");
+            launch(K_RESIZE, [&](){ rehash_kernel<k, l, set_><<<grid_for(total / 32 + 1, 8), 256, 0, stream_>>>(T_, T2, dretry_a_.as<unsigned int>(), dretry_b_.as<unsigned int>(), retried); });
+            std::swap(dretry_a_.p, dretry_b_.p), std::swap(dretry_a_.bytes, dretry_b_.bytes);
+        }
+        sync();
+        std::swap(cs_.p, cs.p), std::swap(cs_.bytes, cs.bytes);
+        std::swap(spill_.p, spill.p), std::swap(spill_.bytes, spill.bytes);
+        std::swap(slots_.p, slots.p), std::swap(slots_.bytes, slots.bytes);
+        std::swap(ov_.p, ov.p), std::swap(ov_.bytes, ov.bytes);
+        bind(T_, cs_, spill_, slots_, new_cap);
+        T_.ov = ov_.as<unsigned long long>(), T_.ov_mask = ov_slots - 1, T_.ov_probe = T2.ov_probe;
+        ov_slots_ = ov_slots;
+        dretry_dirty_ = true;
+    }
+
+    // Sets the overflow count to the occupied slots of T's overflow table.
+    void recount_overflow(const Dev_Table& T, const uint64_t slots)
+    {
+        check(cudaMemsetAsync(ctr() + 1, 0, sizeof(unsigned long long), stream_), "memset");
+        Dev_Table U = T;
+        U.cap = 0;
+        unsigned long long* out = ctr() + 3;
+        check(cudaMemsetAsync(out, 0, 8, stream_), "memset");
+        U.ov_mask = slots - 1;
+        launch(K_OTHER, [&](){ reduce_kernel<true, uint8_t><<<grid_for(slots / 32 + 1, 8), 256, 0, stream_>>>(U, 0, 0, out, 0, nullptr); });
+        check(cudaMemcpyAsync(ctr() + 1, out, 8, cudaMemcpyDeviceToDevice, stream_), "copy");
+    }
+
+    bool dretry_dirty_ = true;
+
+    // ---- Batches ----
+
+    // Stages a host batch: offsets, positions and segments computed here, bases gathered into pinned memory, one
+    // H2D copy.
+    Batch_Info stage_host(const char* const* seqs, const size_t* lens, const size_t n)
+    {
+        uint64_t bytes = 0, nsegs = 0, pos = 0;
+        for(size_t i = 0; i < n; ++i)
+        {
+            bytes += lens[i];
+            const uint64_t p = lens[i] >= size_t(k) ? lens[i] - k + 1 : 0;
+            nsegs += (p + seg_positions - 1) / seg_positions, pos += p;
+        }
+        const size_t o_off = 0, o_pos = o_off + (n + 1) * 8, o_seg = o_pos + (n + 1) * 8, o_bases = o_seg + nsegs * 8;
+        const size_t total = o_bases + bytes + 64;
+        pin_.ensure(total);
+        auto* off = pin_.as<uint64_t>(o_off);
+        auto* pos_off = pin_.as<uint64_t>(o_pos);
+        auto* segs = pin_.as<uint64_t>(o_seg);
+        char* bases = pin_.as<char>(o_bases);
+        uint64_t b = 0, p = 0, g = 0;
+        for(size_t i = 0; i < n; ++i)
+        {
+            off[i] = b, pos_off[i] = p;
+            const uint64_t np = lens[i] >= size_t(k) ? lens[i] - k + 1 : 0;
+            for(uint64_t s = 0; s * seg_positions < np; ++s)
+                segs[g++] = (uint64_t(i) << 24) | s;
+            b += lens[i], p += np;
+        }
+        off[n] = b, pos_off[n] = p;
+        parallel_for(n, 4096, [&](const size_t s, const size_t e)
+        {
+            for(size_t i = s; i < e; ++i)
+                if(lens[i])
+                    std::memcpy(bases + off[i], seqs[i], lens[i]);
+        });
+        dbatch_.ensure(total);
+        check(cudaMemcpyAsync(dbatch_.p, pin_.p, total, cudaMemcpyHostToDevice, stream_), "H2D batch");
+        char* d = dbatch_.as<char>();
+        Batch_Info bi;
+        bi.b = Dev_Batch{reinterpret_cast<const uint8_t*>(d + o_bases), reinterpret_cast<const uint64_t*>(d + o_off),
+                         reinterpret_cast<const uint64_t*>(d + o_seg), reinterpret_cast<const uint64_t*>(d + o_pos), n, nsegs};
+        bi.total_pos = p;
+        return bi;
+    }
+
+    // Prepares a batch already in device memory: positions and segments computed on the device.
+    Batch_Info stage_dev(const uint8_t* bases, const uint64_t* off, const uint64_t n)
+    {
+        const size_t o_npos = 0, o_nseg = o_npos + (n + 1) * 8, o_pos = o_nseg + (n + 1) * 8, o_sego = o_pos + (n + 1) * 8;
+        const size_t head = o_sego + (n + 1) * 8;
+        dtmp_.ensure(head);
+        char* d = dtmp_.as<char>();
+        auto* npos = reinterpret_cast<uint64_t*>(d + o_npos);
+        auto* nseg = reinterpret_cast<uint64_t*>(d + o_nseg);
+        auto* pos_off = reinterpret_cast<uint64_t*>(d + o_pos);
+        auto* seg_off = reinterpret_cast<uint64_t*>(d + o_sego);
+        if(n > 0)
+            launch(K_OTHER, [&](){ batch_counts_kernel<<<(n + 255) / 256, 256, 0, stream_>>>(off, n, k, npos, nseg); });
+        check(cudaMemsetAsync(pos_off, 0, 8, stream_), "memset");
+        check(cudaMemsetAsync(seg_off, 0, 8, stream_), "memset");
+        size_t tmp = 0;
+        if(n > 0)
+        {
+            check(cub::DeviceScan::InclusiveSum(nullptr, tmp, npos, pos_off + 1, static_cast<int64_t>(n), stream_), "scan");
+            dscan_.ensure(tmp);
+            check(cub::DeviceScan::InclusiveSum(dscan_.p, tmp, npos, pos_off + 1, static_cast<int64_t>(n), stream_), "scan");
+            check(cub::DeviceScan::InclusiveSum(dscan_.p, tmp, nseg, seg_off + 1, static_cast<int64_t>(n), stream_), "scan");
+        }
+        pin_ctr_.ensure(64);
+        uint64_t* h = pin_ctr_.as<uint64_t>(32);
+        check(cudaMemcpyAsync(h, pos_off + n, 8, cudaMemcpyDeviceToHost, stream_), "D2H");
+        check(cudaMemcpyAsync(h + 1, seg_off + n, 8, cudaMemcpyDeviceToHost, stream_), "D2H");
+        sync();
+        const uint64_t total_pos = h[0], nsegs = h[1];
+        dbatch_.ensure(nsegs * 8 + 8);
+        if(n > 0)
+            launch(K_OTHER, [&](){ batch_segs_kernel<<<(n + 255) / 256, 256, 0, stream_>>>(seg_off, n, dbatch_.as<uint64_t>()); });
+        Batch_Info bi;
+        bi.b = Dev_Batch{bases, off, dbatch_.as<uint64_t>(), pos_off, n, nsegs};
+        bi.total_pos = total_pos;
+        return bi;
+    }
+
+    template <typename Vis> void stream_launch(const uint32_t kind, const Batch_Info& bi, const uint64_t sb, const uint64_t se, const Vis& vis)
+    {
+        if(se <= sb)
+            return;
+        launch(kind, [&](){ stream_kernel<k, l, Vis><<<grid_for(se - sb, stream_warps), 32 * stream_warps, 0, stream_>>>(bi.b, sb, se, vis); });
+    }
+
+    // The reference's per-user flush accounting over one call (include/Streaming_Kmer_Hash_Table.hpp:2248-2286,
+    // 2511): fed the call's inserted keys chunk by chunk, it doubles the capacity where the reference would.
+    struct Call_Acct
+    {
+        Engine& E;
+        uint32_t user;
+        uint64_t pending, flushed = 0, due, ins_c = 0;
+
+        Call_Acct(Engine& E, const uint32_t u): E(E), user(u), pending(E.pending_[u])
+        {
+            due = pending < E.step_ ? E.step_ - pending : 1;
+        }
+
+        void add(const uint64_t n)
+        {
+            const uint64_t end = ins_c + n;
+            while(due <= end)
+            {
+                const uint64_t at = due;
+                E.approx_sz_ += pending + (at - flushed);
+                pending = 0, flushed = at, due = at + E.step_;
+                if(E.approx_sz_ >= E.resize_th_)
+                {
+                    if(2 * E.cap_ > max_buckets)
+                        throw std::runtime_error("growing the table exceeds the most buckets supported");
+                    E.cap_ *= 2;
+                    E.resize_th_ = static_cast<uint64_t>(static_cast<double>(E.cap_ * B) * E.lf_);
+                    E.step_ = step_for(E.resize_th_);
+                }
+            }
+            ins_c = end;
+        }
+
+        void finish() { E.pending_[user] = pending + (ins_c - flushed); }
+    };
+
+    // Upserts a staged batch with the value functor `fn`, chunk by chunk (see the top of this file).
+    template <typename Fn> uint64_t run_upsert(const uint32_t user, const Batch_Info& bi, const Fn& fn)
+    {
+        Call_Acct acct(*this, user);
+        const uint64_t nsegs = bi.b.nsegs;
+        const double pos_per_seg = nsegs ? static_cast<double>(bi.total_pos) / nsegs : 1.0;
+        uint64_t total_ins = 0;
+        double novelty = 1.0;
+        const size_t bits = bi.total_pos / 8 + 8;
+        unsigned int* retried = reinterpret_cast<unsigned int*>(ctr() + 2);
+
+        for(uint64_t sb = 0; sb < nsegs; )
+        {
+            if(dretry_dirty_ || dretry_a_.bytes < bits || dretry_b_.bytes < bits)
+            {
+                dretry_a_.ensure(bits), dretry_b_.ensure(bits);
+                check(cudaMemsetAsync(dretry_a_.p, 0, dretry_a_.bytes, stream_), "memset");
+                dretry_dirty_ = false;
+            }
+            const double slots = static_cast<double>(cap_ * B);
+            const double room = std::max(0.0, static_cast<double>(resize_th_) - static_cast<double>(size_)) + 0.1 * slots;
+            const double want_pos = room / std::max(novelty, 1e-3);
+            uint64_t se = sb + std::max<uint64_t>(1, static_cast<uint64_t>(want_pos / pos_per_seg));
+            se = std::min(se, nsegs);
+
+            check(cudaMemsetAsync(ctr(), 0, 8, stream_), "memset");
+            check(cudaMemsetAsync(retried, 0, 4, stream_), "memset");
+            Upsert_Visitor<set_, VT, Fn> vis{T_, fn, bi.b.pos_off, ctr(), dretry_a_.as<unsigned int>(), nullptr, retried, 0};
+            stream_launch(K_UPSERT, bi, sb, se, vis);
+            const unsigned long long* c = read_ctr(3);
+            uint64_t ins = c[0];
+            while(static_cast<uint32_t>(c[2]))
+            {
+                grow_overflow();
+                check(cudaMemsetAsync(ctr(), 0, 8, stream_), "memset");
+                check(cudaMemsetAsync(retried, 0, 4, stream_), "memset");
+                check(cudaMemsetAsync(dretry_b_.p, 0, bits, stream_), "memset");
+                Upsert_Visitor<set_, VT, Fn> rv{T_, fn, bi.b.pos_off, ctr(), dretry_b_.as<unsigned int>(), dretry_a_.as<unsigned int>(), retried, 0};
+                stream_launch(K_UPSERT, bi, sb, se, rv);
+                check(cudaMemsetAsync(dretry_a_.p, 0, bits, stream_), "memset");
+                std::swap(dretry_a_.p, dretry_b_.p), std::swap(dretry_a_.bytes, dretry_b_.bytes);
+                c = read_ctr(3);
+                ins += c[0];
+            }
+
+            const double chunk_pos = (se - sb) * pos_per_seg;
+            novelty = chunk_pos > 0 ? std::max(static_cast<double>(ins) / chunk_pos, 1e-3) : novelty;
+            size_ += ins, total_ins += ins;
+            acct.add(ins);
+            const uint64_t gpu_cap = T_.cap;
+            if(cap_ != gpu_cap)
+                resize(cap_);
+            if(c[1] * 4 > ov_slots_ * 3)
+                grow_overflow();
+            sb = se;
+        }
+        acct.finish();
+        return total_ins;
+    }
+
+    template <typename Fn> uint64_t run_update(const Batch_Info& bi, const Fn& fn)
+    {
+        check(cudaMemsetAsync(ctr(), 0, 8, stream_), "memset");
+        Update_Visitor<VT, Fn> vis{T_, fn, ctr(), 0};
+        stream_launch(K_UPDATE, bi, 0, bi.b.nsegs, vis);
+        return read_ctr(3)[0];
+    }
+
+    void run_lookup(const Batch_Info& bi, uint8_t* found, VT* values, uint8_t* fwd)
+    {
+        Lookup_Visitor<set_, VT> vis{T_, bi.b.pos_off, found, values, fwd};
+        stream_launch(K_LOOKUP, bi, 0, bi.b.nsegs, vis);
+    }
+
+    void run_seq_reduce(const Batch_Info& bi, const int mode, const uint64_t mf, const uint64_t mr, unsigned long long* out)
+    {
+        check(cudaMemsetAsync(out, 0, bi.b.n * 8, stream_), "memset");
+        if(mode == 0)
+            stream_launch(K_REDUCE, bi, 0, bi.b.nsegs, Seq_Reduce_Visitor<set_, VT, 0>{T_, out, VT(mf), VT(mr), 0, 0});
+        else if(mode == 1)
+            stream_launch(K_REDUCE, bi, 0, bi.b.nsegs, Seq_Reduce_Visitor<set_, VT, 1>{T_, out, VT(mf), VT(mr), 0, 0});
+        else
+            stream_launch(K_REDUCE, bi, 0, bi.b.nsegs, Seq_Reduce_Visitor<set_, VT, 2>{T_, out, VT(mf), VT(mr), 0, 0});
+    }
+
+    // Copies device output to a host buffer through pinned memory, in pieces, the copy-out overlapping the next D2H.
+    void d2h(void* dst, const void* src, const size_t bytes)
+    {
+        if(bytes == 0)
+            return;
+        const size_t piece = size_t(64) << 20;
+        pin_.ensure(std::min(bytes, 2 * piece));
+        char* stage[2] = {pin_.as<char>(0), pin_.as<char>(std::min(bytes, piece))};
+        for(size_t o = 0, i = 0; o < bytes; o += piece, ++i)
+        {
+            const size_t m = std::min(piece, bytes - o);
+            check(cudaMemcpyAsync(stage[i & 1], static_cast<const char*>(src) + o, m, cudaMemcpyDeviceToHost, stream_), "D2H");
+            sync();
+            parallel_for(m, size_t(4) << 20, [&](const size_t s, const size_t e){ std::memcpy(static_cast<char*>(dst) + o + s, stage[i & 1] + s, e - s); });
+        }
+    }
+
+    static Op_Fn<VT> op_fn(const uint32_t op, const uint64_t x, const uint64_t init) { return Op_Fn<VT>{op, static_cast<VT>(x), static_cast<VT>(init)}; }
+
+public:
+
+    Engine(const uint64_t n, const double lf, const bool pow2):
+          kache_table(k, l, set_ ? 0 : sizeof(VT))
+        , lf_(lf)
+        , cap0_(cap_for(n, lf, pow2))
+        , cap_(cap0_)
+    {
+        if(cap_ > max_buckets)
+            throw std::runtime_error("the table exceeds the most buckets supported");
+        resize_th_ = static_cast<uint64_t>(static_cast<double>(cap_ * B) * lf_);
+        step_ = step_for(resize_th_);
+        int dev = 0;
+        check(cudaGetDevice(&dev), "cudaGetDevice");
+        check(cudaDeviceGetAttribute(&sm_count_, cudaDevAttrMultiProcessorCount, dev), "attribute");
+        check(cudaStreamCreateWithFlags(&own_, cudaStreamNonBlocking), "cudaStreamCreate");
+        stream_ = own_;
+        pin_ctr_.ensure(64);
+        ctr_.ensure(64);
+        check(cudaMemsetAsync(ctr_.p, 0, 64, stream_), "memset");
+        alloc_table(cs_, spill_, slots_, cap_);
+        bind(T_, cs_, spill_, slots_, cap_);
+        // The overflow table starts with room for max(1024, capacity / 32) keys (Streaming_Kmer_Hash_Table.hpp:775).
+        ov_slots_ = ov_slots_for(std::max<uint64_t>(1024, cap_));
+        set_ov(T_, ov_, ov_slots_);
+        sync();
+    }
+
+    ~Engine() override
+    {
+        if(stream_)
+            cudaStreamSynchronize(stream_);
+        for(auto& e : ev_)
+            cudaEventDestroy(e.a), cudaEventDestroy(e.b);
+        if(own_)
+            cudaStreamDestroy(own_);
+    }
+
+    void set_stream(cudaStream_t s) override
+    {
+        std::lock_guard<std::mutex> g(work);
+        sync();
+        stream_ = s ? s : own_;
+    }
+
+    uint64_t upsert(uint32_t user, const char* const* seqs, const size_t* lens, size_t n, uint32_t op, uint64_t x, uint64_t init) override
+    {
+        std::lock_guard<std::mutex> g(work);
+        const auto bi = stage_host(seqs, lens, n);
+        return run_upsert(user, bi, op_fn(op, x, init));
+    }
+
+    uint64_t upsert_oriented(uint32_t user, const char* const* seqs, const size_t* lens, size_t n, uint32_t op, uint64_t xf, uint64_t xr) override
+    {
+        if constexpr(set_)
+            return 0;
+        else
+        {
+            std::lock_guard<std::mutex> g(work);
+            const auto bi = stage_host(seqs, lens, n);
+            return run_upsert(user, bi, Oriented_Op_Fn<VT>{op, static_cast<VT>(xf), static_cast<VT>(xr)});
+        }
+    }
+
+    uint64_t update(const char* const* seqs, const size_t* lens, size_t n, uint32_t op, uint64_t x) override
+    {
+        if constexpr(set_)
+            return 0;
+        else
+        {
+            std::lock_guard<std::mutex> g(work);
+            const auto bi = stage_host(seqs, lens, n);
+            return run_update(bi, op_fn(op, x, 0));
+        }
+    }
+
+    void lookup(const char* const* seqs, const size_t* lens, size_t n, uint8_t* found, void* values, uint8_t* fwd) override
+    {
+        std::lock_guard<std::mutex> g(work);
+        const auto bi = stage_host(seqs, lens, n);
+        const uint64_t P = bi.total_pos;
+        const size_t vb = (!set_ && values) ? sizeof(VT) : 0;
+        const size_t a_found = (P + 15) / 16 * 16, a_val = (P * vb + 15) / 16 * 16;
+        dout_.ensure(a_found + a_val + P + 64);
+        uint8_t* d_found = dout_.as<uint8_t>();
+        VT* d_val = vb ? reinterpret_cast<VT*>(d_found + a_found) : nullptr;
+        uint8_t* d_fwd = fwd ? d_found + a_found + a_val : nullptr;
+        run_lookup(bi, d_found, d_val, d_fwd);
+        d2h(found, d_found, P);
+        if(vb)
+            d2h(values, d_val, P * vb);
+        if(fwd)
+            d2h(fwd, d_fwd, P);
+    }
+
+    void seq_reduce(const char* const* seqs, const size_t* lens, size_t n, int mode, uint64_t m_fwd, uint64_t m_rev, uint64_t* out) override
+    {
+        std::lock_guard<std::mutex> g(work);
+        const auto bi = stage_host(seqs, lens, n);
+        dout_.ensure(n * 8 + 8);
+        run_seq_reduce(bi, mode, m_fwd, m_rev, dout_.as<unsigned long long>());
+        d2h(out, dout_.p, n * 8);
+    }
+
+    void describe(const char* const* seqs, const size_t* lens, size_t n, uint64_t* key, uint64_t* h, uint8_t* cs, uint8_t* fwd, uint8_t* valid) override
+    {
+        std::lock_guard<std::mutex> g(work);
+        const auto bi = stage_host(seqs, lens, n);
+        const uint64_t P = bi.total_pos;
+        dout_.ensure(P * 19 + 64);
+        auto* dk = dout_.as<uint64_t>();
+        auto* dh = dk + P;
+        auto* dc = reinterpret_cast<uint8_t*>(dh + P);
+        stream_launch(K_OTHER, bi, 0, bi.b.nsegs, Describe_Visitor{bi.b.pos_off, dk, dh, dc, dc + P, dc + 2 * P});
+        d2h(key, dk, P * 8), d2h(h, dh, P * 8), d2h(cs, dc, P), d2h(fwd, dc + P, P), d2h(valid, dc + 2 * P, P);
+    }
+
+    uint64_t upsert_dev(uint32_t user, const uint8_t* b, const uint64_t* off, uint64_t n, uint32_t op, uint64_t x, uint64_t init) override
+    {
+        std::lock_guard<std::mutex> g(work);
+        const auto bi = stage_dev(b, off, n);
+        return run_upsert(user, bi, op_fn(op, x, init));
+    }
+
+    uint64_t upsert_oriented_dev(uint32_t user, const uint8_t* b, const uint64_t* off, uint64_t n, uint32_t op, uint64_t xf, uint64_t xr) override
+    {
+        if constexpr(set_)
+            return 0;
+        else
+        {
+            std::lock_guard<std::mutex> g(work);
+            const auto bi = stage_dev(b, off, n);
+            return run_upsert(user, bi, Oriented_Op_Fn<VT>{op, static_cast<VT>(xf), static_cast<VT>(xr)});
+        }
+    }
+
+    uint64_t update_dev(const uint8_t* b, const uint64_t* off, uint64_t n, uint32_t op, uint64_t x) override
+    {
+        if constexpr(set_)
+            return 0;
+        else
+        {
+            std::lock_guard<std::mutex> g(work);
+            const auto bi = stage_dev(b, off, n);
+            return run_update(bi, op_fn(op, x, 0));
+        }
+    }
+
+    void lookup_dev(const uint8_t* b, const uint64_t* off, uint64_t n, uint8_t* found, void* values, uint8_t* fwd) override
+    {
+        std::lock_guard<std::mutex> g(work);
+        const auto bi = stage_dev(b, off, n);
+        run_lookup(bi, found, set_ ? nullptr : static_cast<VT*>(values), fwd);
+        sync();
+    }
+
+    void count_dev(const uint8_t* b, const uint64_t* off, uint64_t n, uint64_t* counts) override
+    {
+        std::lock_guard<std::mutex> g(work);
+        const auto bi = stage_dev(b, off, n);
+        run_seq_reduce(bi, 0, 0, 0, reinterpret_cast<unsigned long long*>(counts));
+        sync();
+    }
+
+    bool get(const char* kmer, uint64_t& value) override
+    {
+        value = 0;
+        uint64_t f = 0;
+        for(int i = 0; i < k; ++i)
+        {
+            if(!host_acgt(kmer[i]))
+                return false;
+            f = (f << 2) | static_cast<uint64_t>(((kmer[i] >> 2) ^ (kmer[i] >> 1)) & 3);
+        }
+        uint64_t r = 0, y = f;
+        for(int i = 0; i < k; ++i, y >>= 2)
+            r = (r << 2) | (3 - (y & 3));
+        const uint64_t key = f < r ? f : r;
+        std::lock_guard<std::mutex> g(work);
+        auto* h = pin_ctr_.as<uint64_t>(0);
+        h[0] = key;
+        unsigned long long* d = ctr() + 4;
+        check(cudaMemcpyAsync(d, h, 8, cudaMemcpyHostToDevice, stream_), "H2D");
+        launch(K_OTHER, [&](){ get_kernel<k, l, set_, VT><<<1, 32, 0, stream_>>>(T_, reinterpret_cast<const uint64_t*>(d), 1, d + 1); });
+        check(cudaMemcpyAsync(h + 1, d + 1, 16, cudaMemcpyDeviceToHost, stream_), "D2H");
+        sync();
+        value = h[2];
+        return h[1] != 0;
+    }
+
+    uint64_t size() const override { return size_; }
+    uint64_t capacity() const override { return cap_ * B; }
+
+    uint64_t reduce(uint32_t what, uint64_t mask) override
+    {
+        std::lock_guard<std::mutex> g(work);
+        unsigned long long* out = ctr() + 3;
+        check(cudaMemsetAsync(out, 0, 8, stream_), "memset");
+        const uint64_t total = cap_ * B + ov_slots_;
+        launch(K_OTHER, [&](){ reduce_kernel<set_, VT><<<grid_for(total / 32 + 1, 8), 256, 0, stream_>>>(T_, what, mask, out, 0, nullptr); });
+        return read_ctr(4)[3];
+    }
+
+    void histogram(uint64_t max, uint64_t* h) override
+    {
+        std::lock_guard<std::mutex> g(work);
+        dout_.ensure((max + 1) * 8);
+        check(cudaMemsetAsync(dout_.p, 0, (max + 1) * 8, stream_), "memset");
+        const uint64_t total = cap_ * B + ov_slots_;
+        launch(K_OTHER, [&](){ reduce_kernel<set_, VT><<<grid_for(total / 32 + 1, 8), 256, 0, stream_>>>(T_, 3, 0, ctr() + 3, max, dout_.as<unsigned long long>()); });
+        d2h(h, dout_.p, (max + 1) * 8);
+        h[0] = 0;
+    }
+
+    void for_each(uint32_t shards, uint32_t shard, kache_keys_fn f, void* ctx) override
+    {
+        std::lock_guard<std::mutex> g(work);
+        const uint64_t bb = cap_ * shard / shards, be = cap_ * (shard + 1) / shards;
+        const uint64_t ov_range = (ov_slots_ + shards - 1) / shards;
+        const uint64_t ob = std::min<uint64_t>(ov_range * shard, ov_slots_), oe = std::min<uint64_t>(ov_range * (shard + 1), ov_slots_);
+        constexpr uint64_t piece = uint64_t(1) << 18;   // Buckets per device pass.
+        constexpr size_t chunk = 4096;                  // Keys per callback (capi/Kmer_Table.hpp:234).
+        std::vector<uint64_t> K, Vv;
+        std::vector<VT> W(set_ ? 0 : chunk);
+        bool done = false;
+        const auto pass = [&](const uint64_t b0, const uint64_t b1, const uint64_t o0, const uint64_t o1)
+        {
+            const uint64_t slots = (b1 - b0) * B + (o1 - o0);
+            if(slots == 0 || done)
+                return;
+            dout_.ensure(slots * 16 + 64);
+            uint64_t* dk = dout_.as<uint64_t>();
+            uint64_t* dv = set_ ? nullptr : dk + slots;
+            unsigned long long* cnt = ctr() + 3;
+            check(cudaMemsetAsync(cnt, 0, 8, stream_), "memset");
+            launch(K_OTHER, [&](){ collect_kernel<set_><<<grid_for(slots / 32 + 1, 8), 256, 0, stream_>>>(T_, b0, b1, o0, o1, dk, dv, cnt); });
+            const uint64_t m = read_ctr(4)[3];
+            K.resize(m), Vv.resize(set_ ? 0 : m);
+            d2h(K.data(), dk, m * 8);
+            if(!set_)
+                d2h(Vv.data(), dv, m * 8);
+            for(uint64_t s = 0; s < m && !done; s += chunk)
+            {
+                const size_t c = std::min<uint64_t>(chunk, m - s);
+                if constexpr(!set_)
+                    for(size_t i = 0; i < c; ++i)
+                        W[i] = static_cast<VT>(Vv[s + i]);
+                done = f(ctx, K.data() + s, set_ ? nullptr : static_cast<const void*>(W.data()), c) != 0;
+            }
+        };
+        for(uint64_t b = bb; b < be && !done; b += piece)
+            pass(b, std::min(be, b + piece), 0, 0);
+        for(uint64_t o = ob; o < oe && !done; o += piece * B)
+            pass(0, 0, o, std::min(oe, o + piece * B));
+    }
+
+    void get_stats(kache_stats& out) override
+    {
+        std::lock_guard<std::mutex> g(work);
+        out = kache_stats{};
+        out.capacity = cap_ * B;
+        out.bytes = cap_ * (B + 32 + B * slot_bytes);
+        out.keys = size_;
+        unsigned long long* ps = ctr() + 3;
+        check(cudaMemsetAsync(ps, 0, 16, stream_), "memset");
+        launch(K_OTHER, [&](){ distribution_kernel<k, l, set_><<<grid_for(cap_ * B / 32 + 1, 8), 256, 0, stream_>>>(T_, ps); });
+        const auto* c = read_ctr(5);
+        out.overflow_keys = c[1];
+        const double p = static_cast<double>(c[3]), s = static_cast<double>(c[4]), o = static_cast<double>(c[1]);
+        if(out.keys > 0)
+        {
+            const double t = p + s + o;
+            out.primary_pct = p * 100.0 / t, out.secondary_pct = s * 100.0 / t, out.overflow_pct = o * 100.0 / t;
+        }
+    }
+
+    // Empties the table, back to its initial capacity and sizing state; registrations stay.
+    void clear() override
+    {
+        std::lock_guard<std::mutex> g(work);
+        if(T_.cap != cap0_)
+        {
+            alloc_table(cs_, spill_, slots_, cap0_);
+            bind(T_, cs_, spill_, slots_, cap0_);
+            ov_slots_ = ov_slots_for(std::max<uint64_t>(1024, cap0_));
+            set_ov(T_, ov_, ov_slots_);
+        }
+        else
+        {
+            check(cudaMemsetAsync(cs_.p, 0, cap0_ * B, stream_), "memset");
+            check(cudaMemsetAsync(spill_.p, 0, cap0_ * 32, stream_), "memset");
+            check(cudaMemsetAsync(slots_.p, 0, cap0_ * B * slot_bytes, stream_), "memset");
+            check(cudaMemsetAsync(ov_.p, 0, ov_slots_ * 32, stream_), "memset");
+        }
+        check(cudaMemsetAsync(ctr(), 0, 64, stream_), "memset");
+        cap_ = cap0_;
+        resize_th_ = static_cast<uint64_t>(static_cast<double>(cap_ * B) * lf_);
+        step_ = step_for(resize_th_);
+        approx_sz_ = 0, size_ = 0;
+        std::fill(pending_, pending_ + KACHE_MAX_USERS, 0);
+    }
+
+    void profile(bool on) override
+    {
+        std::lock_guard<std::mutex> g(work);
+        sync();
+        for(auto& e : ev_)
+            cudaEventDestroy(e.a), cudaEventDestroy(e.b);
+        ev_.clear();
+        std::fill(prof_ms_, prof_ms_ + K_KINDS, 0.0), std::fill(prof_n_, prof_n_ + K_KINDS, 0);
+        prof_ = on;
+    }
+
+    void profile_read(uint32_t kind, double& ms, uint64_t& n) override
+    {
+        std::lock_guard<std::mutex> g(work);
+        sync();
+        for(auto& e : ev_)
+        {
+            float t = 0;
+            check(cudaEventElapsedTime(&t, e.a, e.b), "elapsed");
+            prof_ms_[e.kind] += t, prof_n_[e.kind]++;
+            cudaEventDestroy(e.a), cudaEventDestroy(e.b);
+        }
+        ev_.clear();
+        ms = kind < K_KINDS ? prof_ms_[kind] : 0, n = kind < K_KINDS ? prof_n_[kind] : 0;
+    }
+};
+
+}

@@ -185,6 +185,40 @@ double now_s() { return std::chrono::duration<double>(std::chrono::steady_clock:
 }
 
 
+// The reference's batch describer (include/Kmer_Batch.hpp) over a sequence split into ACGT stretches
+// (include/DNA_Utility.hpp:199-224), per position: canonical key, minimizer hash, checksum, orientation, validity;
+// and the lane describer's minimizer hashes recomputed from the keys (include/Kmer_Lanes.hpp:247-274).
+template <uint16_t k, uint16_t l>
+uint64_t describe_with(const char* s, uint64_t len, uint64_t* key, uint64_t* h, uint8_t* cs, uint8_t* fwd, uint8_t* valid, uint64_t* h_lanes)
+{
+    if(len < k)
+        return 0;
+    const uint64_t n = len - k + 1;
+    std::fill(key, key + n, 0), std::fill(h, h + n, 0), std::fill(cs, cs + n, 0), std::fill(fwd, fwd + n, 0), std::fill(valid, valid + n, 0);
+    std::fill(h_lanes, h_lanes + n, 0);
+    typedef Kmer_Batch<k, l> batch_t;
+    batch_t kb;
+    typename batch_t::Oriented_Chunk ch;
+    for(uint64_t st = 0; st + k <= len; )
+    {
+        const uint64_t e = st + DNA_Utility::acgt_prefix(s + st, len - st);
+        if(e - st >= k)
+        {
+            kb.reset(s + st, e - st - (k - 1));
+            uint64_t at = st;
+            while(kb.next(ch))
+            {
+                for(std::size_t i = 0; i < ch.n; ++i)
+                    key[at + i] = ch.key[i], h[at + i] = ch.h[i], cs[at + i] = ch.c[i], fwd[at + i] = ch.o[i], valid[at + i] = 1;
+                Kmer_Lanes<k, l>::minimizer_hashes(ch.key, ch.n, h_lanes + at);
+                at += ch.n;
+            }
+        }
+        st = e + 1;
+    }
+    return n;
+}
+
 extern "C"
 {
 
@@ -221,6 +255,17 @@ uint64_t ref_size(void* t) { return static_cast<Table*>(t)->size(); }
 uint64_t ref_capacity(void* t) { return static_cast<Table*>(t)->capacity(); }
 uint64_t ref_overflow_size(void* t) { return static_cast<Table*>(t)->overflow_size(); }
 uint64_t ref_dump(void* t, uint64_t* keys, uint64_t* vals) { return static_cast<Table*>(t)->dump(keys, vals, 1, 0); }
+
+uint64_t ref_describe(uint32_t k, const char* s, uint64_t len, uint64_t* key, uint64_t* h, uint8_t* cs, uint8_t* fwd, uint8_t* valid, uint64_t* h_lanes)
+{
+    switch(k)
+    {
+    case 31: return describe_with<31, 22>(s, len, key, h, cs, fwd, valid, h_lanes);
+    case 27: return describe_with<27, 16>(s, len, key, h, cs, fwd, valid, h_lanes);
+    case 32: return describe_with<32, 20>(s, len, key, h, cs, fwd, valid, h_lanes);
+    default: return 0;
+    }
+}
 
 // The CPU baseline's drivers, as the reference's benchmark drives its table (benchmark/measure.cpp:45-140,
 // benchmark/harness.hpp:268-303): batches of `batch` sequences handed to `threads` users round-robin. Return

@@ -47,6 +47,20 @@ int kache_b200_update_dev(kache_table* t, const uint8_t* d_bases, const uint64_t
 int kache_b200_lookup_dev(kache_table* t, const uint8_t* d_bases, const uint64_t* d_off, uint64_t n, uint8_t* d_found, void* d_values, uint8_t* d_fwd) KACHE_NOEXCEPT;
 int kache_b200_count_dev(kache_table* t, const uint8_t* d_bases, const uint64_t* d_off, uint64_t n, uint64_t* d_counts) KACHE_NOEXCEPT;
 
+/* kache_b200_count_dev for callers that cannot allocate device memory: no counterpart in the reference.
+ *
+ * Callers running inside their own memory pool, inside a CUDA graph capture, or in a process that budgets every byte
+ * of HBM itself cannot let the library call cudaMalloc on a query. This entry point allocates nothing: its scratch
+ * (the batch's segment list) lives in one fixed 8 MiB device array that every GPU which loads the library holds until
+ * the process exits. It takes at most KACHE_B200_NOALLOC_MAX_SEGMENTS sequences and as many segments of up to 512
+ * k-mer positions; beyond that it returns KACHE_EINVAL (up front when n is over the limit, after the kernels when
+ * the segments are). Tables of 31-mers with 22-minimizers only (those of kache_new). Every call shares the array and
+ * clears its header first, so calls whose GPU work overlaps (other streams or threads) race: serialise them. The
+ * first call on a device looks the array's device address up (cudaGetSymbolAddress); make that first call before
+ * any stream capture. The call returns synchronised with the table's stream. */
+#define KACHE_B200_NOALLOC_MAX_SEGMENTS 1048544ull
+int kache_b200_count_dev_noalloc(kache_table* t, const uint8_t* d_bases, const uint64_t* d_off, uint64_t n, uint64_t* d_counts) KACHE_NOEXCEPT;
+
 /* The describer's output per position, laid out as kache_lookup's: canonical key, minimizer hash, checksum,
  * orientation, whether the k characters are all ACGT. For checking the describer against the reference's. */
 int kache_b200_describe(kache_table* t, const char* const* seqs, const size_t* lens, size_t n, uint64_t* key, uint64_t* h, uint8_t* cs, uint8_t* fwd, uint8_t* valid) KACHE_NOEXCEPT;

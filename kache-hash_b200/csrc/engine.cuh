@@ -57,6 +57,9 @@ struct kache_table
     virtual void histogram(uint64_t max, uint64_t* h) = 0;
     virtual void get_stats(kache_stats& out) = 0;
     virtual void clear() = 0;
+    // The table's device view and stream, for entry points that launch their own kernels on it.
+    virtual kache_b200::Dev_Table device_table() const = 0;
+    virtual cudaStream_t stream() const = 0;
     virtual void profile(bool on) = 0;
     virtual void profile_read(uint32_t kind, double& ms, uint64_t& launches) = 0;
 };
@@ -891,6 +894,9 @@ public:
             out.primary_pct = p * 100.0 / t, out.secondary_pct = s * 100.0 / t, out.overflow_pct = o * 100.0 / t;
         }
     }
+
+    Dev_Table device_table() const override { return T_; }
+    cudaStream_t stream() const override { return stream_; }
 
     // Empties the table, back to its initial capacity and sizing state; registrations stay.
     void clear() override

@@ -218,8 +218,9 @@ def run_b200(args):
         step_dev()
     barrier()
     clocks = Clocks(local)
-    clocks.start()
-    time.sleep(0.3)
+    if not args.only_dev:
+        clocks.start()
+        time.sleep(0.3)
     launches0 = kache.kernel_launches()
     T.profile(True)
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -232,7 +233,7 @@ def run_b200(args):
     launches = kache.kernel_launches() - launches0
     prof = {kind: T.profile_read(i) for i, kind in enumerate(["upsert", "update", "lookup", "reduce", "resize", "other"])}
     T.profile(False)
-    clk = clocks.stop()
+    clk = clocks.stop() if not args.only_dev else None
 
     # Per-kernel roofline: algorithmic bytes per launch over the kernel's mean event-timed duration.
     st = T.stats()
@@ -259,14 +260,16 @@ def run_b200(args):
     d = kernels[dom]
 
     # End to end through the C interface with host buffers.
-    for _ in range(max(1, args.warmup // 2)):
-        step_e2e()
-    barrier()
-    t0 = time.perf_counter()
-    for _ in range(args.steps):
-        step_e2e()
-    barrier()
-    e2e_ms = max_over_ranks((time.perf_counter() - t0) * 1000) / args.steps
+    e2e_ms = float("nan")
+    if not args.only_dev:
+        for _ in range(max(1, args.warmup // 2)):
+            step_e2e()
+        barrier()
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            step_e2e()
+        barrier()
+        e2e_ms = max_over_ranks((time.perf_counter() - t0) * 1000) / args.steps
 
     if rank == 0:
         line = {
@@ -287,7 +290,7 @@ def run_b200(args):
                     "d2h_bytes_per_step": int(P_find * 9)},
             "clocks": clk,
         }
-        cb = cpu_baseline_sample(ins, held, min(128, os.cpu_count() or 1))
+        cb = None if args.only_dev else cpu_baseline_sample(ins, held, min(128, os.cpu_count() or 1))
         line["cpu_baseline"] = cb
         print(json.dumps(line))
     T.close()
@@ -318,6 +321,8 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--only-dev", action="store_true",
+                    help="time the device-resident steps only (no e2e, CPU baseline or clock sampling): the profiling case")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)

@@ -81,6 +81,12 @@ int kache_b200_profile_read(kache_table* t, uint32_t kind, double* ms, uint64_t*
 /* Kernels this library has launched in this process, over all tables. */
 uint64_t kache_b200_kernel_launches(void) KACHE_NOEXCEPT;
 
+/* Reads the FASTA or FASTQ file (or pipe) at `path` and calls f(ctx, seqs, lens, n) with its non-empty sequences in
+ * order, in batches of whole sequences of about `batch_bases` bases, until f returns nonzero
+ * (counter/Fastx_Reader.hpp:13-52). Unreadable, gzip-compressed or malformed input returns KACHE_EINVAL. */
+typedef int (*kache_seqs_fn)(void* ctx, const char* const* seqs, const size_t* lens, size_t n);
+int kache_b200_fastx_read(const char* path, uint64_t batch_bases, kache_seqs_fn f, void* ctx) KACHE_NOEXCEPT;
+
 /* The counter library (counter/Kmer_Set_Counter.hpp:23-76): a set of 31-mers primed at count 0 and counted by
  * present-only increments that wrap at 2^32. Paths name FASTA or FASTQ files, or pipes. */
 typedef struct kache_counter kache_counter;

@@ -53,7 +53,23 @@ def build(force=False, verbose=False):
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError(f"link failed:\n{r.stderr}")
+    build_facade_check(headers, force)
     return LIB
+
+
+def build_facade_check(headers, force=False):
+    """The C++ template surface's check program (tests/facade_check.cu), linked against the library."""
+    src = os.path.join(ROOT, "tests", "facade_check.cu")
+    exe = os.path.join(OUT, "facade_check")
+    if not os.path.exists(src):
+        return None
+    if not force and os.path.exists(exe) and os.path.getmtime(exe) >= max(_newest(headers), os.path.getmtime(src), os.path.getmtime(LIB)):
+        return exe
+    cmd = [NVCC] + ARCH + FLAGS + [src, "-o", exe, "-L" + OUT, "-lkache_b200", "-Xlinker", "-rpath=" + OUT]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError(f"nvcc failed on {src}:\n{r.stderr}")
+    return exe
 
 
 if __name__ == "__main__":

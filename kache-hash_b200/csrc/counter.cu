@@ -48,6 +48,10 @@ int guard(const F& f) noexcept
     {
         return KACHE_ENOMEM;
     }
+    catch(const Cuda_Error&)
+    {
+        return KACHE_EINTERNAL;
+    }
     catch(const std::runtime_error&)
     {
         return KACHE_EINVAL;    // Unreadable or malformed input; the reference throws std::runtime_error.
@@ -198,6 +202,28 @@ int kache_counter_size(kache_counter* const c, uint64_t* const n) noexcept
     if(c == nullptr || n == nullptr)
         return KACHE_EINVAL;
     return guard([&](){ return *n = c->t->size(), KACHE_OK; });
+}
+
+int kache_b200_fastx_read(const char* const path, const uint64_t batch, const kache_seqs_fn f, void* const ctx) noexcept
+{
+    if(path == nullptr || f == nullptr || batch == 0)
+        return KACHE_EINVAL;
+    return guard([&]()
+    {
+        Fastx_Reader r(path);
+        std::vector<char> bases;
+        std::vector<size_t> lens;
+        std::vector<const char*> seqs;
+        while(r.next(bases, lens, batch))
+        {
+            seqs.resize(lens.size());
+            for(size_t i = 0, o = 0; i < lens.size(); o += lens[i], ++i)
+                seqs[i] = bases.data() + o;
+            if(f(ctx, seqs.data(), lens.data(), lens.size()) != 0)
+                break;
+        }
+        return KACHE_OK;
+    });
 }
 
 kache_table* kache_counter_table(kache_counter* const c) noexcept

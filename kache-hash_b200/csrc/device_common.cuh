@@ -26,15 +26,19 @@ constexpr int seg_positions = 32 * seg_rows;
 
 enum Op : uint32_t { OP_KEEP = 0, OP_ASSIGN = 1, OP_ADD = 2, OP_OR = 3, OP_MIN = 4, OP_MAX = 5, OP_ADD_WRAP = 16 };
 
+// Wang's hash with its shift-and-add steps written as multiplications by constants, modulo 2^64:
+// ~x + (x << 21) = x * (2^21 - 1) - 1, x + (x << 3) + (x << 8) = x * 265, x + (x << 2) + (x << 4) = x * 21,
+// x + (x << 31) = x * (2^31 + 1). Same value; the multiplies run on the FMA pipe, leaving the integer ALU pipe,
+// which the describer saturates, to the shifts and XORs.
 __host__ __device__ __forceinline__ uint64_t wang_u64(uint64_t x)
 {
-    x = (~x) + (x << 21);
+    x = x * ((1ull << 21) - 1) - 1;
     x = x ^ (x >> 24);
-    x = (x + (x << 3)) + (x << 8);
+    x = x * 265;
     x = x ^ (x >> 14);
-    x = (x + (x << 2)) + (x << 4);
+    x = x * 21;
     x = x ^ (x >> 28);
-    x = x + (x << 31);
+    x = x * ((1ull << 31) + 1);
     return x;
 }
 
@@ -121,20 +125,33 @@ __device__ __forceinline__ uint64_t spread32(const uint32_t x)
     return v;
 }
 
+// Bit 7 of each byte of the result is set iff that byte of w is zero, exactly (no carries cross bytes).
+__device__ __forceinline__ uint32_t zero_bytes(const uint32_t w)
+{
+    return ~(((w & 0x7F7F7F7Fu) + 0x7F7F7F7Fu) | w) & 0x80808080u;
+}
+
+// Gathers bits 7, 15, 23, 31 of y into bits 0..3.
+__device__ __forceinline__ uint32_t gather4(const uint32_t y)
+{
+    return (((y >> 7) * 0x00204081u) >> 21) & 0xFu;
+}
+
 // Bit j of the result is set iff byte j of the 32 bytes (a, b) equals c.
 __device__ __forceinline__ uint32_t match32(const uint4 a, const uint4 b, const uint32_t c)
 {
     const uint32_t cc = c * 0x01010101u;
-    uint32_t m = 0;
     const uint32_t w[8] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w};
+    uint32_t y[8], any = 0;
 #pragma unroll
     for(int i = 0; i < 8; ++i)
-    {
-        const uint32_t e = __vcmpeq4(w[i], cc);   // 0xFF per equal byte
-        // Compress the four byte-masks to four bits.
-        const uint32_t bits = ((e >> 7) & 1) | ((e >> 14) & 2) | ((e >> 21) & 4) | ((e >> 28) & 8);
-        m |= bits << (4 * i);
-    }
+        y[i] = zero_bytes(w[i] ^ cc), any |= y[i];
+    if(!any)
+        return 0;
+    uint32_t m = 0;
+#pragma unroll
+    for(int i = 0; i < 8; ++i)
+        m |= gather4(y[i]) << (4 * i);
     return m;
 }
 

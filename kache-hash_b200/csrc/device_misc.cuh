@@ -9,7 +9,7 @@ namespace kache_b200
 {
 
 // Inserts one key with its value, known absent (every key of a table is distinct), into `T`. Returns INSERTED or
-// OV_FULL.
+// OV_FULL. No other thread inserts the same key, so none waits for the value: no fence before publishing.
 template <bool set_>
 __device__ __forceinline__ uint32_t place_key(const Dev_Table& T, const uint64_t key, const uint64_t h, const unsigned long long val)
 {
@@ -19,7 +19,7 @@ __device__ __forceinline__ uint32_t place_key(const Dev_Table& T, const uint64_t
     {
         if constexpr(!set_)
             *L.val = val;
-        publish(L, !set_);
+        publish(L, false);
         if(!L.cs)
             atomicAdd(T.ov_count, 1ull);
     }
@@ -60,6 +60,55 @@ __global__ void __launch_bounds__(256) rehash_kernel(const Dev_Table from, const
         {
             atomicOr(retry_out + (s >> 5), 1u << (s & 31));
             *retried = 1;
+        }
+    }
+}
+
+// Resize, first phase (include/Streaming_Kmer_Hash_Table.hpp:1494-1570, out of place): a warp per old bucket b.
+// The keys whose primary bucket is b move to their primary bucket in the new table, one of the 2^d buckets
+// [b * 2^d, (b + 1) * 2^d) when the capacity grows 2^d-fold, since bucket_of is monotone in the capacity; the warp
+// writes each of those buckets whole (checksums, keys, values, a cleared spill filter), so the new arrays need no
+// clearing. Keys held in b as a secondary bucket get their bit set in `rest`, for the second phase (rehash_kernel).
+template <int k, int l, bool set_>
+__global__ void __launch_bounds__(256) split_kernel(const Dev_Table from, const Dev_Table to, const uint32_t d, unsigned int* rest)
+{
+    const uint32_t lane = threadIdx.x & 31;
+    const uint64_t warps = uint64_t(gridDim.x) * (blockDim.x / 32);
+    for(uint64_t b = uint64_t(blockIdx.x) * (blockDim.x / 32) + (threadIdx.x >> 5); b < from.cap; b += warps)
+    {
+        const uint64_t s = b * B + lane;
+        const uint8_t c = from.cs[s];
+        unsigned long long key_st = 0, val = 0;
+        uint32_t dest = 0xFFFFFFFFu;
+        if(c)
+        {
+            key_st = from.slots[s * slot_words<set_>()];
+            if constexpr(!set_)
+                val = from.slots[s * 2 + 1];
+            const uint64_t h = minimizer_hash<k, l>(~key_st);
+            if(bucket_of(h, from.cap) == b)
+                dest = static_cast<uint32_t>(bucket_of(h, to.cap) - (b << d));
+        }
+        const uint32_t other = __ballot_sync(0xFFFFFFFFu, c != 0 && dest == 0xFFFFFFFFu);
+        if(lane == 0 && other)
+            rest[s >> 5] = other;   // s >> 5 == b: one word per old bucket.
+        for(uint32_t t = 0; t < (1u << d); ++t)
+        {
+            const uint32_t m = __ballot_sync(0xFFFFFFFFu, dest == t);
+            const uint64_t nb = (b << d) + t;
+            // Lane j writes slot j of the new bucket: the rank-j key moving there, or an empty slot.
+            const uint32_t n = __popc(m);
+            const uint32_t src = lane < n ? __fns(m, 0, static_cast<int>(lane) + 1) : 0;
+            const unsigned long long k_j = __shfl_sync(0xFFFFFFFFu, key_st, src);
+            const unsigned long long v_j = __shfl_sync(0xFFFFFFFFu, val, src);
+            const uint32_t c_j = __shfl_sync(0xFFFFFFFFu, static_cast<uint32_t>(c), src);
+            const uint64_t ns = nb * B + lane;
+            to.slots[ns * slot_words<set_>()] = lane < n ? k_j : 0ull;
+            if constexpr(!set_)
+                to.slots[ns * 2 + 1] = lane < n ? v_j : 0ull;
+            to.cs[ns] = lane < n ? static_cast<uint8_t>(c_j) : 0;
+            if(lane < 8)
+                to.spill[nb * 8 + lane] = 0;
         }
     }
 }

@@ -59,14 +59,23 @@ __device__ __forceinline__ Row load_row(const uint8_t* seq, const uint64_t len, 
     return r;
 }
 
-// The forward and reverse-complement n-mers (n <= 32) starting at base j of row a, spilling into row b.
+// The forward and reverse-complement n-mers (n <= 32) starting at base j of row a, spilling into row b: 64-bit
+// windows of the 128-bit pairs (a.W, b.W) and (b.R, a.R) at bit offset 2j, as two 32-bit funnel shifts each; which
+// words feed them depends on the lane only (j >= 16).
 template <int n>
 __device__ __forceinline__ void window(const Row& a, const Row& b, const uint32_t j, uint64_t& f, uint64_t& r)
 {
-    const uint32_t s = 2 * j;
-    const uint64_t top = (a.W << s) | ((b.W >> (63 - s)) >> 1);
+    const bool big = j >= 16;
+    const uint32_t sh = (2 * j) & 31;
+    const uint32_t a1 = static_cast<uint32_t>(a.W >> 32), a0 = static_cast<uint32_t>(a.W);
+    const uint32_t b1 = static_cast<uint32_t>(b.W >> 32), b0 = static_cast<uint32_t>(b.W);
+    const uint32_t x3 = big ? a0 : a1, x2 = big ? b1 : a0, x1 = big ? b0 : b1;
+    const uint64_t top = (uint64_t(__funnelshift_l(x2, x3, sh)) << 32) | __funnelshift_l(x1, x2, sh);
     f = top >> (64 - 2 * n);
-    const uint64_t low = (a.R >> s) | ((b.R << (63 - s)) << 1);
+    const uint32_t r0 = static_cast<uint32_t>(a.R), r1 = static_cast<uint32_t>(a.R >> 32);
+    const uint32_t r2 = static_cast<uint32_t>(b.R), r3 = static_cast<uint32_t>(b.R >> 32);
+    const uint32_t y0 = big ? r1 : r0, y1 = big ? r2 : r1, y2 = big ? r3 : r2;
+    const uint64_t low = (uint64_t(__funnelshift_r(y1, y2, sh)) << 32) | __funnelshift_r(y0, y1, sh);
     r = low & kmer_mask(n);
 }
 
@@ -180,6 +189,8 @@ struct Upsert_Visitor
     __device__ __forceinline__ void begin() { ins = 0; }
     __device__ __forceinline__ void begin_segment(uint64_t) {}
     __device__ __forceinline__ void end_segment(uint64_t, uint32_t) {}
+    __device__ __forceinline__ void lane_begin(uint64_t, bool) {}
+    __device__ __forceinline__ void lane_end(uint64_t, bool) {}
 
     __device__ __forceinline__ void visit(const Kmer_Desc& d, const uint32_t lane)
     {
@@ -194,11 +205,17 @@ struct Upsert_Visitor
         uint32_t r = NONE;
         if(active)
             r = upsert_chain<set_>(T, d.key, d.h, d.c, L);
+        const bool comm = fn.commutes();
         if(r == INSERTED)
         {
             if constexpr(!set_)
-                write_val<V>(L.val, fn.initial(d.fwd));
-            publish(L, !set_);
+            {
+                if(comm)
+                    fn.apply_init(L.val, d.fwd);
+                else
+                    write_val<V>(L.val, fn.initial(d.fwd));
+            }
+            publish(L, !set_ && !comm);
         }
         else if(r == OV_FULL)
         {
@@ -212,7 +229,7 @@ struct Upsert_Visitor
         if constexpr(!set_)
             if((r == FOUND || r == FOUND_PENDING) && !fn.is_noop())
             {
-                if(r == FOUND_PENDING && !await_published(L))
+                if(r == FOUND_PENDING && !comm && !await_published(L))
                     atomicOr(T.err, ERR_WAIT);
                 fn.apply(L.val, d.fwd);
             }
@@ -235,6 +252,8 @@ struct Update_Visitor
     __device__ __forceinline__ void begin() { cnt = 0; }
     __device__ __forceinline__ void begin_segment(uint64_t) {}
     __device__ __forceinline__ void end_segment(uint64_t, uint32_t) {}
+    __device__ __forceinline__ void lane_begin(uint64_t, bool) {}
+    __device__ __forceinline__ void lane_end(uint64_t, bool) {}
 
     __device__ __forceinline__ void visit(const Kmer_Desc& d, const uint32_t)
     {
@@ -259,10 +278,13 @@ struct Lookup_Visitor
     uint8_t* found;
     V* values;
     uint8_t* fwd;
+    uint64_t obase;
 
     __device__ __forceinline__ void begin() {}
-    __device__ __forceinline__ void begin_segment(uint64_t) {}
+    __device__ __forceinline__ void begin_segment(const uint64_t q) { obase = pos_off[q]; }
     __device__ __forceinline__ void end_segment(uint64_t, uint32_t) {}
+    __device__ __forceinline__ void lane_begin(const uint64_t q, const bool has) { obase = has ? pos_off[q] : 0; }
+    __device__ __forceinline__ void lane_end(uint64_t, bool) {}
     __device__ __forceinline__ void end(uint32_t) {}
 
     __device__ __forceinline__ void visit(const Kmer_Desc& d, const uint32_t)
@@ -272,7 +294,7 @@ struct Lookup_Visitor
             v = find_chain<set_, false>(T, d.key, d.h, d.c);
         if(!d.in)
             return;
-        const uint64_t o = pos_off[d.q] + d.pos;
+        const uint64_t o = obase + d.pos;
         found[o] = d.valid ? (v ? 1 : 0) : 2;
         if constexpr(!set_)
             if(values)
@@ -319,6 +341,13 @@ struct Seq_Reduce_Visitor
             atomicAdd(out + q, a);
         total += a;
     }
+    // One lane, one sequence's segment: its own total.
+    __device__ __forceinline__ void lane_begin(uint64_t, bool) { acc = 0; }
+    __device__ __forceinline__ void lane_end(const uint64_t q, const bool has)
+    {
+        if(has && acc)
+            atomicAdd(out + q, acc);
+    }
     __device__ __forceinline__ void end(uint32_t) {}
 };
 
@@ -335,6 +364,8 @@ struct Describe_Visitor
     __device__ __forceinline__ void begin() {}
     __device__ __forceinline__ void begin_segment(uint64_t) {}
     __device__ __forceinline__ void end_segment(uint64_t, uint32_t) {}
+    __device__ __forceinline__ void lane_begin(uint64_t, bool) {}
+    __device__ __forceinline__ void lane_end(uint64_t, bool) {}
     __device__ __forceinline__ void end(uint32_t) {}
     __device__ __forceinline__ void visit(const Kmer_Desc& d, const uint32_t)
     {

@@ -133,6 +133,21 @@ struct Op_Fn
     __device__ __forceinline__ V initial(bool) const { return init; }
     __device__ __forceinline__ bool is_noop() const { return op == OP_KEEP; }
 
+    // Whether every update of a key combines with the others in any order, starting from a zeroed value: then an
+    // inserter folds its initial value in atomically (op(0, init) = init for these ops) and nobody waits for it.
+    __device__ __forceinline__ bool commutes() const
+    {
+        return op == OP_KEEP || op == OP_ADD || op == OP_ADD_WRAP || op == OP_OR || op == OP_MAX;
+    }
+
+    __device__ __forceinline__ void apply_init(unsigned long long* w, bool) const
+    {
+        if(op == OP_KEEP)
+            write_val<V>(w, init);
+        else
+            Op_Fn<V>{op, init, init}.apply(w, true);
+    }
+
     __device__ __forceinline__ void apply(unsigned long long* w, bool) const
     {
         if(op == OP_KEEP)
@@ -179,6 +194,8 @@ struct Oriented_Op_Fn
     __device__ __forceinline__ Op_Fn<V> at(const bool fwd) const { return Op_Fn<V>{op, fwd ? x_fwd : x_rev, V(0)}; }
     __device__ __forceinline__ V initial(const bool fwd) const { return at(fwd)(V(0)); }
     __device__ __forceinline__ bool is_noop() const { return false; }
+    __device__ __forceinline__ bool commutes() const { return op == OP_ADD || op == OP_ADD_WRAP || op == OP_OR || op == OP_MAX; }
+    __device__ __forceinline__ void apply_init(unsigned long long* w, const bool fwd) const { at(fwd).apply(w, fwd); }
     __device__ __forceinline__ void apply(unsigned long long* w, const bool fwd) const { at(fwd).apply(w, fwd); }
 };
 
@@ -190,6 +207,8 @@ struct User_Fn
     V val;
     __device__ __forceinline__ V initial(bool) const { return val; }
     __device__ __forceinline__ bool is_noop() const { return false; }
+    __device__ __forceinline__ bool commutes() const { return false; }
+    __device__ __forceinline__ void apply_init(unsigned long long* w, bool) const { write_val<V>(w, val); }
     __device__ __forceinline__ void apply(unsigned long long* w, bool) const { cas_update<V>(w, f); }
 };
 
@@ -200,6 +219,8 @@ struct User_Oriented_Fn
     F f;
     __device__ __forceinline__ V initial(const bool fwd) const { return f(V(), fwd); }
     __device__ __forceinline__ bool is_noop() const { return false; }
+    __device__ __forceinline__ bool commutes() const { return false; }
+    __device__ __forceinline__ void apply_init(unsigned long long* w, const bool fwd) const { write_val<V>(w, f(V(), fwd)); }
     __device__ __forceinline__ void apply(unsigned long long* w, const bool fwd) const
     {
         const F& g = f;

@@ -10,6 +10,7 @@
 #pragma once
 
 #include "device_misc.cuh"
+#include "device_lanes.cuh"
 #include "kache_capi.h"
 
 #include <cub/device/device_scan.cuh>
@@ -326,8 +327,15 @@ class Engine final : public kache_table
     {
         if(new_cap > max_buckets)
             throw std::runtime_error("the table would exceed the most buckets supported");
+        const uint64_t old_cap = T_.cap;
+        uint32_t d = 0;
+        while((old_cap << d) < new_cap)
+            d++;
+        if((old_cap << d) != new_cap)
+            throw std::logic_error("a resize multiplies the bucket count by a power of 2");
+        // The new buckets are written whole by split_kernel: no clearing.
         Dev_Buf cs, spill, slots, ov;
-        alloc_table(cs, spill, slots, new_cap);
+        cs.ensure(new_cap * B), spill.ensure(new_cap * 32), slots.ensure(new_cap * B * slot_bytes);
         Dev_Table T2{};
         bind(T2, cs, spill, slots, new_cap);
         const uint64_t ov_keys = read_ctr(2)[1];
@@ -336,12 +344,18 @@ class Engine final : public kache_table
         // The keys move, so the overflow count starts over.
         check(cudaMemsetAsync(ctr() + 1, 0, sizeof(unsigned long long), stream_), "memset");
 
-        const uint64_t total = cap_ * B + ov_slots_;
+        // First phase: keys at their primary buckets move directly. Second phase: the others and the overflow
+        // table's keys, marked in `dretry_a_`, go through the insertion chain.
+        const uint64_t main_slots = old_cap * B, total = main_slots + ov_slots_;
         dretry_a_.ensure(total / 8 + 8), dretry_b_.ensure(total / 8 + 8);
-        check(cudaMemsetAsync(dretry_a_.p, 0, total / 8 + 8, stream_), "memset");
+        check(cudaMemsetAsync(dretry_a_.p, 0, main_slots / 8, stream_), "memset");
+        check(cudaMemsetAsync(dretry_a_.as<char>() + main_slots / 8, 0xFF, ov_slots_ / 8, stream_), "memset");
         unsigned int* retried = reinterpret_cast<unsigned int*>(ctr() + 2);
         check(cudaMemsetAsync(retried, 0, 4, stream_), "memset");
-        launch(K_RESIZE, [&](){ rehash_kernel<k, l, set_><<<grid_for(total / 32 + 1, 8), 256, 0, stream_>>>(T_, T2, nullptr, dretry_a_.as<unsigned int>(), retried); });
+        check(cudaMemsetAsync(dretry_b_.p, 0, total / 8 + 8, stream_), "memset");
+        launch(K_RESIZE, [&](){ split_kernel<k, l, set_><<<grid_for(old_cap, 8), 256, 0, stream_>>>(T_, T2, d, dretry_a_.as<unsigned int>()); });
+        launch(K_RESIZE, [&](){ rehash_kernel<k, l, set_><<<grid_for(total / 32 + 1, 8), 256, 0, stream_>>>(T_, T2, dretry_a_.as<unsigned int>(), dretry_b_.as<unsigned int>(), retried); });
+        std::swap(dretry_a_.p, dretry_b_.p), std::swap(dretry_a_.bytes, dretry_b_.bytes);
         while(static_cast<uint32_t>(read_ctr(3)[2]))
         {
             // The new overflow table filled up: double it, then retry the keys that found it full.
@@ -387,6 +401,7 @@ class Engine final : public kache_table
     }
 
     bool dretry_dirty_ = true;
+    std::vector<uint64_t> seg_hist_;
 
     // ---- Batches ----
 
@@ -408,16 +423,34 @@ class Engine final : public kache_table
         auto* pos_off = pin_.as<uint64_t>(o_pos);
         auto* segs = pin_.as<uint64_t>(o_seg);
         char* bases = pin_.as<char>(o_bases);
-        uint64_t b = 0, p = 0, g = 0;
+        // Segments listed longest first (a counting sort by length), so that the 32 lanes of a warp, which step as
+        // long as their longest segment, get segments of similar lengths.
+        seg_hist_.assign(seg_positions + 1, 0);
+        uint64_t b = 0, p = 0;
         for(size_t i = 0; i < n; ++i)
         {
             off[i] = b, pos_off[i] = p;
             const uint64_t np = lens[i] >= size_t(k) ? lens[i] - k + 1 : 0;
-            for(uint64_t s = 0; s * seg_positions < np; ++s)
-                segs[g++] = (uint64_t(i) << 24) | s;
+            if(np)
+                seg_hist_[seg_positions] += np / seg_positions, seg_hist_[np % seg_positions]++;
             b += lens[i], p += np;
         }
         off[n] = b, pos_off[n] = p;
+        seg_hist_[0] = 0;
+        for(uint64_t len = seg_positions, at = 0; len > 0; --len)
+        {
+            const uint64_t c = seg_hist_[len];
+            seg_hist_[len] = at, at += c;
+        }
+        for(size_t i = 0; i < n; ++i)
+        {
+            const uint64_t np = lens[i] >= size_t(k) ? lens[i] - k + 1 : 0;
+            for(uint64_t s = 0; s * seg_positions < np; ++s)
+            {
+                const uint64_t len = std::min<uint64_t>(np - s * seg_positions, seg_positions);
+                segs[seg_hist_[len]++] = (uint64_t(i) << 24) | s;
+            }
+        }
         parallel_for(n, 4096, [&](const size_t s, const size_t e)
         {
             for(size_t i = s; i < e; ++i)
@@ -472,11 +505,21 @@ class Engine final : public kache_table
         return bi;
     }
 
-    template <typename Vis> void stream_launch(const uint32_t kind, const Batch_Info& bi, const uint64_t sb, const uint64_t se, const Vis& vis)
+    // Operations without per-position output (upsert, update, per-sequence reductions) run one lane per segment
+    // (device_lanes.cuh): rolling descriptions, and lanes of a warp on different reads. Lookups and descriptions, whose
+    // outputs are per position, run one warp per segment (device_stream.cuh), so that a row's 32 outputs are written
+    // as one coalesced store.
+    template <typename Vis> void stream_launch(const uint32_t kind, const Batch_Info& bi, const uint64_t sb, const uint64_t se, const Vis& vis, const bool per_position = false)
     {
         if(se <= sb)
             return;
-        launch(kind, [&](){ stream_kernel<k, l, Vis><<<grid_for(se - sb, stream_warps), 32 * stream_warps, 0, stream_>>>(bi.b, sb, se, vis); });
+        if(per_position)
+        {
+            launch(kind, [&](){ stream_kernel<k, l, Vis><<<grid_for(se - sb, stream_warps), 32 * stream_warps, 0, stream_>>>(bi.b, sb, se, vis); });
+            return;
+        }
+        const uint64_t blocks = std::min<uint64_t>((se - sb + lane_block - 1) / lane_block, uint64_t(sm_count_) * 8);
+        launch(kind, [&](){ lane_kernel<k, l, Vis><<<static_cast<unsigned>(blocks), lane_block, 0, stream_>>>(bi.b, sb, se, vis); });
     }
 
     // The reference's per-user flush accounting over one call (include/Streaming_Kmer_Hash_Table.hpp:2248-2286,
@@ -585,8 +628,8 @@ class Engine final : public kache_table
 
     void run_lookup(const Batch_Info& bi, uint8_t* found, VT* values, uint8_t* fwd)
     {
-        Lookup_Visitor<set_, VT> vis{T_, bi.b.pos_off, found, values, fwd};
-        stream_launch(K_LOOKUP, bi, 0, bi.b.nsegs, vis);
+        Lookup_Visitor<set_, VT> vis{T_, bi.b.pos_off, found, values, fwd, 0};
+        stream_launch(K_LOOKUP, bi, 0, bi.b.nsegs, vis, true);
     }
 
     void run_seq_reduce(const Batch_Info& bi, const int mode, const uint64_t mf, const uint64_t mr, unsigned long long* out)
@@ -732,7 +775,7 @@ public:
         auto* dk = dout_.as<uint64_t>();
         auto* dh = dk + P;
         auto* dc = reinterpret_cast<uint8_t*>(dh + P);
-        stream_launch(K_OTHER, bi, 0, bi.b.nsegs, Describe_Visitor{bi.b.pos_off, dk, dh, dc, dc + P, dc + 2 * P});
+        stream_launch(K_OTHER, bi, 0, bi.b.nsegs, Describe_Visitor{bi.b.pos_off, dk, dh, dc, dc + P, dc + 2 * P}, true);
         d2h(key, dk, P * 8), d2h(h, dh, P * 8), d2h(cs, dc, P), d2h(fwd, dc + P, P), d2h(valid, dc + 2 * P, P);
     }
 
@@ -893,6 +936,22 @@ public:
             const double t = p + s + o;
             out.primary_pct = p * 100.0 / t, out.secondary_pct = s * 100.0 / t, out.overflow_pct = o * 100.0 / t;
         }
+    }
+
+    // Upsert and update with any value functor (the C++ template facade's user functors: User_Fn,
+    // User_Oriented_Fn), from a host batch.
+    template <typename Fn> uint64_t upsert_with(const uint32_t user, const char* const* seqs, const size_t* lens, const size_t n, const Fn& fn)
+    {
+        std::lock_guard<std::mutex> g(work);
+        const auto bi = stage_host(seqs, lens, n);
+        return run_upsert(user, bi, fn);
+    }
+
+    template <typename Fn> uint64_t update_with(const char* const* seqs, const size_t* lens, const size_t n, const Fn& fn)
+    {
+        std::lock_guard<std::mutex> g(work);
+        const auto bi = stage_host(seqs, lens, n);
+        return run_update(bi, fn);
     }
 
     Dev_Table device_table() const override { return T_; }

@@ -311,5 +311,69 @@ class Table:
         return ms.value, n.value
 
 
+class Counter:
+    """The counter library (counter/Kmer_Set_Counter.hpp): 31-mers primed at count 0, counted by +1 per occurrence."""
+
+    def __init__(self, n, threads=1, load_factor=0.9, k=31):
+        L = lib()
+        for name, args in (("kache_counter_new", [ctypes.c_uint32, ctypes.c_uint64, ctypes.c_uint32, ctypes.c_double, ctypes.POINTER(_vp)]),
+                           ("kache_counter_free", [_vp]), ("kache_counter_prime", [_vp, ctypes.c_char_p]),
+                           ("kache_counter_count", [_vp, ctypes.c_char_p, _u64p]),
+                           ("kache_counter_prime_batch", [_vp, _vp, _vp, ctypes.c_size_t]),
+                           ("kache_counter_count_batch", [_vp, _vp, _vp, ctypes.c_size_t, _u64p]),
+                           ("kache_counter_histogram", [_vp, ctypes.c_uint64, _vp]),
+                           ("kache_counter_count_of", [_vp, ctypes.c_char_p, _u64p]),
+                           ("kache_counter_size", [_vp, _u64p]), ("kache_counter_table", [_vp])):
+            f = getattr(L, name)
+            f.argtypes = args
+            f.restype = None if name == "kache_counter_free" else (_vp if name == "kache_counter_table" else ctypes.c_int)
+        h = _vp()
+        _check(L.kache_counter_new(k, n, threads, load_factor, ctypes.byref(h)), "kache_counter_new")
+        self.h = h
+
+    def close(self):
+        if self.h:
+            lib().kache_counter_free(self.h)
+            self.h = _vp()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def prime(self, path):
+        _check(lib().kache_counter_prime(self.h, path.encode()), "kache_counter_prime")
+
+    def count(self, path):
+        r = ctypes.c_uint64()
+        _check(lib().kache_counter_count(self.h, path.encode(), ctypes.byref(r)), "kache_counter_count")
+        return r.value
+
+    def prime_batch(self, b):
+        _check(lib().kache_counter_prime_batch(self.h, *b.args()), "kache_counter_prime_batch")
+
+    def count_batch(self, b):
+        r = ctypes.c_uint64()
+        _check(lib().kache_counter_count_batch(self.h, *b.args(), ctypes.byref(r)), "kache_counter_count_batch")
+        return r.value
+
+    def histogram(self, max_count):
+        h = np.zeros(max_count + 1, np.uint64)
+        _check(lib().kache_counter_histogram(self.h, max_count, h.ctypes.data), "kache_counter_histogram")
+        return h
+
+    def count_of(self, kmer):
+        r = ctypes.c_uint64()
+        kmer = kmer.encode() if isinstance(kmer, str) else kmer
+        _check(lib().kache_counter_count_of(self.h, kmer, ctypes.byref(r)), "kache_counter_count_of")
+        return r.value
+
+    def size(self):
+        r = ctypes.c_uint64()
+        _check(lib().kache_counter_size(self.h, ctypes.byref(r)), "kache_counter_size")
+        return r.value
+
+
 def kernel_launches():
     return lib().kache_b200_kernel_launches()

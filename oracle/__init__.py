@@ -181,6 +181,8 @@ REF_KINDS = {(31, 8): 0, (31, 4): 1, (31, 2): 2, (31, 1): 3, (31, 0): 4, (27, 1)
 
 
 def ref_lib_path():
+    if os.environ.get("KACHE_REF_LIB"):
+        return os.environ["KACHE_REF_LIB"]
     v4 = os.path.join(REF_DIR, "libkache_ref_v4.so")
     v3 = os.path.join(REF_DIR, "libkache_ref_v3.so")
     if _cpu_has_avx512() and os.path.exists(v4):

@@ -88,13 +88,29 @@ def dist_env():
     return ws, rank, local
 
 
-def workload(rank):
-    g, ins, held = synth.config1()
+def rank_seeds(rank):
+    """The read seeds of a rank: rank 0 runs the workload itself; each other rank its own reads of the same shape,
+    into its own table (weak scaling over independent tables)."""
+    return (11, 2) if rank == 0 else (11 + 100 * rank, 2 + 100 * rank)
+
+
+def workload(rank, scale=1.0):
+    g, ins, held = synth.config1(scale)
     if rank:
-        # Each rank its own reads of the same shape (weak scaling).
-        ins = synth.reads_fixed(g, 333_333, 150, seed=11 + 100 * rank)
-        held = synth.reads_fixed(g, 1_000_000, 150, seed=2 + 100 * rank)
+        s_ins, s_held = rank_seeds(rank)
+        ins = synth.reads_fixed(g, int(333_333 * scale), 150, seed=s_ins)
+        held = synth.reads_fixed(g, int(1_000_000 * scale), 150, seed=s_held)
     return ins, held
+
+
+def max_over_ranks(dist, x, device):
+    """The largest of the ranks' values (the job's time is its slowest rank's)."""
+    if dist is None:
+        return x
+    import torch
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
 
 
 def positions(off, k=31):
@@ -206,13 +222,6 @@ def run_b200(args):
             dist.barrier()
         torch.cuda.synchronize()
 
-    def max_over_ranks(x):
-        if dist is None:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
-
     # Device-resident: warm-up, then exactly `steps` steps between barriers, timed with CUDA events on the stream.
     for _ in range(args.warmup):
         step_dev()
@@ -229,7 +238,7 @@ def run_b200(args):
         step_dev()
     e1.record(stream)
     barrier()
-    ms = max_over_ranks(e0.elapsed_time(e1)) / args.steps
+    ms = max_over_ranks(dist, e0.elapsed_time(e1), dev) / args.steps
     launches = kache.kernel_launches() - launches0
     prof = {kind: T.profile_read(i) for i, kind in enumerate(["upsert", "update", "lookup", "reduce", "resize", "other"])}
     T.profile(False)
@@ -269,7 +278,7 @@ def run_b200(args):
         for _ in range(args.steps):
             step_e2e()
         barrier()
-        e2e_ms = max_over_ranks((time.perf_counter() - t0) * 1000) / args.steps
+        e2e_ms = max_over_ranks(dist, (time.perf_counter() - t0) * 1000, dev) / args.steps
 
     if rank == 0:
         line = {

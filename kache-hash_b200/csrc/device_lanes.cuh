@@ -38,7 +38,7 @@ __global__ void __launch_bounds__(lane_block) lane_kernel(const Dev_Batch batch,
     {
         const uint64_t g = g0 + lane;
         const bool has = g < seg_e;
-        uint64_t q = 0, p0 = 0;
+        uint64_t q = 0, p0 = 0, obase = 0;
         uint32_t npos = 0, steps = 0;
         const uint8_t* p = nullptr;
         if(has)
@@ -47,6 +47,7 @@ __global__ void __launch_bounds__(lane_block) lane_kernel(const Dev_Batch batch,
             q = packed >> 24;
             const uint64_t b0 = batch.off[q], len = batch.off[q + 1] - b0;
             p0 = (packed & 0xFFFFFF) * seg_positions;
+            obase = batch.pos_off[q] + p0;
             npos = static_cast<uint32_t>(min(len - k + 1 - p0, static_cast<uint64_t>(seg_positions)));
             p = batch.bases + b0 + p0;
             steps = npos + k - 1;
@@ -92,6 +93,8 @@ __global__ void __launch_bounds__(lane_block) lane_kernel(const Dev_Batch batch,
             const uint32_t i = t + 1 - k;
             d.q = q;
             d.pos = p0 + i;
+            d.out = obase + i;
+            d.last = false;
             d.in = i < npos;
             d.valid = d.in && run >= static_cast<uint32_t>(k);
             d.key = min64(kf, kr);

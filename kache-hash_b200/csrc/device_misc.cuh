@@ -26,41 +26,65 @@ __device__ __forceinline__ uint32_t place_key(const Dev_Table& T, const uint64_t
     return r;
 }
 
-// Resize (include/Streaming_Kmer_Hash_Table.hpp:1474-1681, out of place): every key of the old table, from its
-// buckets and its overflow table, goes into the new one; minimizer hashes are recomputed from the keys
-// (include/Streaming_Kmer_Hash_Table.hpp:1459-1470). A thread per old slot. Keys that find the new overflow table
-// full set their bit in `retry_out`; with `retry_in`, only those run.
+// Resize, second phase: the old slots marked in `marks` (keys not at their primary bucket, and the overflow table's
+// slots) go through the insertion chain of the new table. A warp takes 32 words of marks (1024 slots), lists their set
+// bits in shared memory, and then works through the list a slot per lane, so that lanes stay busy however sparse the
+// marks are. Keys that find the new overflow table full set their bit in `retry_out`.
 template <int k, int l, bool set_>
-__global__ void __launch_bounds__(256) rehash_kernel(const Dev_Table from, const Dev_Table to, const unsigned int* retry_in, unsigned int* retry_out, unsigned int* retried)
+__global__ void __launch_bounds__(256) rest_kernel(const Dev_Table from, const Dev_Table to, const unsigned int* marks, const uint64_t total,
+                                                   unsigned int* retry_out, unsigned int* retried)
 {
-    const uint64_t main_slots = from.cap * B, total = main_slots + from.ov_mask + 1;
-    for(uint64_t s = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; s < total; s += uint64_t(gridDim.x) * blockDim.x)
+    __shared__ uint16_t list_all[8][1024];
+    const uint32_t lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    uint16_t* list = list_all[wid];
+    const uint64_t main_slots = from.cap * B, words = (total + 31) / 32;
+    const uint64_t warps = uint64_t(gridDim.x) * 8;
+    for(uint64_t wb = uint64_t(blockIdx.x) * 8 + wid; wb * 32 < words; wb += warps)
     {
-        if(retry_in && !((retry_in[s >> 5] >> (s & 31)) & 1))
-            continue;
-        unsigned long long key_st, val = 0;
-        if(s < main_slots)
+        const uint64_t wi = wb * 32 + lane;
+        uint32_t word = wi < words ? marks[wi] : 0u;
+        if(wi * 32 + 32 > total && wi < words)
+            word &= (total - wi * 32) >= 32 ? ~0u : ((1u << (total - wi * 32)) - 1);
+        const uint32_t cnt = __popc(word);
+        uint32_t pre = cnt;
+#pragma unroll
+        for(int o = 1; o < 32; o <<= 1)
         {
-            if(from.cs[s] == 0)
-                continue;
-            key_st = from.slots[s * slot_words<set_>()];
-            if constexpr(!set_)
-                val = from.slots[s * 2 + 1];
+            const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, pre, o);
+            if(lane >= static_cast<uint32_t>(o))
+                pre += y;
         }
-        else
+        const uint32_t n = __shfl_sync(0xFFFFFFFFu, pre, 31);
+        pre -= cnt;
+        for(uint32_t w = word, i = pre; w; w &= w - 1, ++i)
+            list[i] = static_cast<uint16_t>(lane * 32 + __ffs(w) - 1);
+        __syncwarp();
+        for(uint32_t r = lane; r < n; r += 32)
         {
-            const uint64_t i = s - main_slots;
-            key_st = from.ov[4 * i];
+            const uint64_t s = wb * 1024 + list[r];
+            unsigned long long key_st, val = 0;
+            if(s < main_slots)
+            {
+                key_st = from.slots[s * slot_words<set_>()];
+                if constexpr(!set_)
+                    val = from.slots[s * 2 + 1];
+            }
+            else
+            {
+                const uint64_t i = s - main_slots;
+                key_st = from.ov[4 * i];
+                val = from.ov[4 * i + 1];
+            }
             if(key_st == 0)
                 continue;
-            val = from.ov[4 * i + 1];
+            const uint64_t key = ~key_st;
+            if(place_key<set_>(to, key, minimizer_hash<k, l>(key), val) == OV_FULL)
+            {
+                atomicOr(retry_out + (s >> 5), 1u << (s & 31));
+                *retried = 1;
+            }
         }
-        const uint64_t key = ~key_st;
-        if(place_key<set_>(to, key, minimizer_hash<k, l>(key), val) == OV_FULL)
-        {
-            atomicOr(retry_out + (s >> 5), 1u << (s & 31));
-            *retried = 1;
-        }
+        __syncwarp();
     }
 }
 
@@ -68,7 +92,7 @@ __global__ void __launch_bounds__(256) rehash_kernel(const Dev_Table from, const
 // The keys whose primary bucket is b move to their primary bucket in the new table, one of the 2^d buckets
 // [b * 2^d, (b + 1) * 2^d) when the capacity grows 2^d-fold, since bucket_of is monotone in the capacity; the warp
 // writes each of those buckets whole (checksums, keys, values, a cleared spill filter), so the new arrays need no
-// clearing. Keys held in b as a secondary bucket get their bit set in `rest`, for the second phase (rehash_kernel).
+// clearing. Keys held in b as a secondary bucket get their bit set in `rest`, for the second phase (rest_kernel).
 template <int k, int l, bool set_>
 __global__ void __launch_bounds__(256) split_kernel(const Dev_Table from, const Dev_Table to, const uint32_t d, unsigned int* rest)
 {

@@ -84,10 +84,12 @@ struct Kmer_Desc
 {
     uint64_t key, h;
     uint64_t q, pos;    // Sequence and position in it.
+    uint64_t out;       // Index of the position in the batch's outputs (set by the lane kernel; 0 in the warp kernel).
     uint8_t c;
     bool fwd;           // Occurs as its canonical form.
     bool valid;         // All k characters are ACGT.
     bool in;            // The position exists (is in the segment).
+    bool last;          // Unused; false.
 };
 
 template <int k, int l, typename Visitor>
@@ -137,6 +139,7 @@ __global__ void __launch_bounds__(32 * stream_warps) stream_kernel(const Dev_Bat
             const uint64_t vbits = ((uint64_t(r1.valid) << 32) | r0.valid) >> lane;
             const uint64_t km = (k == 32 ? 0xFFFFFFFFull : (1ull << k) - 1);
             d.pos = p0 + 32 * r + lane;
+            d.out = 0, d.last = false;
             d.q = q;
             d.in = d.pos < p1;
             d.valid = d.in && (vbits & km) == km;
@@ -185,8 +188,10 @@ struct Upsert_Visitor
     const unsigned int* retry_in;
     unsigned int* retried;      // Set to 1 if any bit of retry_out was set.
     unsigned long long ins;
+    static constexpr int stage_bytes = 0;
 
     __device__ __forceinline__ void begin() { ins = 0; }
+    __device__ __forceinline__ void begin(uint8_t*) { ins = 0; }
     __device__ __forceinline__ void begin_segment(uint64_t) {}
     __device__ __forceinline__ void end_segment(uint64_t, uint32_t) {}
     __device__ __forceinline__ void lane_begin(uint64_t, bool) {}
@@ -197,7 +202,7 @@ struct Upsert_Visitor
         bool active = d.valid;
         if(retry_in && active)
         {
-            const uint64_t gpos = pos_off[d.q] + d.pos;
+            const uint64_t gpos = d.out;
             active = (retry_in[gpos >> 5] >> (gpos & 31)) & 1;
         }
 
@@ -219,7 +224,7 @@ struct Upsert_Visitor
         }
         else if(r == OV_FULL)
         {
-            const uint64_t gpos = pos_off[d.q] + d.pos;
+            const uint64_t gpos = d.out;
             atomicOr(retry_out + (gpos >> 5), 1u << (gpos & 31));
             *retried = 1;
         }
@@ -248,8 +253,10 @@ struct Update_Visitor
     Fn fn;
     unsigned long long* present;
     unsigned long long cnt;
+    static constexpr int stage_bytes = 0;
 
     __device__ __forceinline__ void begin() { cnt = 0; }
+    __device__ __forceinline__ void begin(uint8_t*) { cnt = 0; }
     __device__ __forceinline__ void begin_segment(uint64_t) {}
     __device__ __forceinline__ void end_segment(uint64_t, uint32_t) {}
     __device__ __forceinline__ void lane_begin(uint64_t, bool) {}
@@ -314,8 +321,10 @@ struct Seq_Reduce_Visitor
     V m_fwd, m_rev;
     unsigned long long acc;
     unsigned long long total;
+    static constexpr int stage_bytes = 0;
 
     __device__ __forceinline__ void begin() { total = 0; }
+    __device__ __forceinline__ void begin(uint8_t*) { total = 0; }
     __device__ __forceinline__ void begin_segment(uint64_t) { acc = 0; }
     __device__ __forceinline__ void visit(const Kmer_Desc& d, const uint32_t)
     {
@@ -360,8 +369,11 @@ struct Describe_Visitor
     uint8_t* cs;
     uint8_t* fwd;
     uint8_t* valid;
+    bool by_out;    // Outputs at d.out (the lane kernel) rather than pos_off[q] + pos.
+    static constexpr int stage_bytes = 0;
 
     __device__ __forceinline__ void begin() {}
+    __device__ __forceinline__ void begin(uint8_t*) {}
     __device__ __forceinline__ void begin_segment(uint64_t) {}
     __device__ __forceinline__ void end_segment(uint64_t, uint32_t) {}
     __device__ __forceinline__ void lane_begin(uint64_t, bool) {}
@@ -371,7 +383,7 @@ struct Describe_Visitor
     {
         if(!d.in)
             return;
-        const uint64_t o = pos_off[d.q] + d.pos;
+        const uint64_t o = by_out ? d.out : pos_off[d.q] + d.pos;
         key[o] = d.valid ? d.key : 0, h[o] = d.valid ? d.h : 0, cs[o] = d.valid ? d.c : 0;
         fwd[o] = d.valid && d.fwd, valid[o] = d.valid;
     }

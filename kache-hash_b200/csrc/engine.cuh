@@ -18,6 +18,8 @@
 #include <algorithm>
 #include <atomic>
 #include <cmath>
+#include <condition_variable>
+#include <functional>
 #include <cstring>
 #include <mutex>
 #include <new>
@@ -175,21 +177,94 @@ struct Pinned_Buf
     template <typename T> T* as(size_t byte_off = 0) const { return reinterpret_cast<T*>(static_cast<char*>(p) + byte_off); }
 };
 
-// Copies on up to `t_c` threads; small copies stay on this one.
-inline void parallel_for(const size_t n, const size_t min_per_thread, const auto& f)
+// A pool of host threads, started once, for the copies between callers' buffers and pinned staging memory.
+class Host_Pool
 {
-    const size_t hw = std::max(1u, std::thread::hardware_concurrency());
-    const size_t t_c = std::min<size_t>(std::min<size_t>(hw, 32), std::max<size_t>(1, n / std::max<size_t>(1, min_per_thread)));
-    if(t_c <= 1)
+    std::vector<std::thread> W_;
+    std::mutex run_mu_, mu_;
+    std::condition_variable cv_, done_cv_;
+    const std::function<void(size_t, size_t)>* job_ = nullptr;
+    size_t n_ = 0, parts_ = 0, finished_ = 0;
+    std::atomic<size_t> next_{0};
+    uint64_t gen_ = 0;
+    bool stop_ = false;
+
+    void work_parts()
     {
-        f(size_t(0), n);
-        return;
+        for(size_t p; (p = next_++) < parts_; )
+        {
+            (*job_)(n_ * p / parts_, n_ * (p + 1) / parts_);
+            std::lock_guard<std::mutex> g(mu_);
+            if(++finished_ == parts_)
+                done_cv_.notify_all();
+        }
     }
-    std::vector<std::thread> W;
-    for(size_t t = 0; t < t_c; ++t)
-        W.emplace_back([&, t](){ f(n * t / t_c, n * (t + 1) / t_c); });
-    for(auto& w : W)
-        w.join();
+
+    Host_Pool()
+    {
+        const size_t t_c = std::min<size_t>(31, std::max(1u, std::thread::hardware_concurrency()) - 1);
+        for(size_t t = 0; t < t_c; ++t)
+            W_.emplace_back([this]()
+            {
+                uint64_t seen = 0;
+                while(true)
+                {
+                    {
+                        std::unique_lock<std::mutex> g(mu_);
+                        cv_.wait(g, [&](){ return stop_ || gen_ != seen; });
+                        if(stop_)
+                            return;
+                        seen = gen_;
+                    }
+                    work_parts();
+                }
+            });
+    }
+
+public:
+
+    ~Host_Pool()
+    {
+        {
+            std::lock_guard<std::mutex> g(mu_);
+            stop_ = true;
+        }
+        cv_.notify_all();
+        for(auto& w : W_)
+            w.join();
+    }
+
+    static Host_Pool& get()
+    {
+        static Host_Pool pool;
+        return pool;
+    }
+
+    // Runs f(s, e) over [0, n) in parts of at least `min_part`, on the pool and this thread; returns when all ran.
+    void run(const size_t n, const size_t min_part, const std::function<void(size_t, size_t)>& f)
+    {
+        const size_t parts = std::min<size_t>(4 * (W_.size() + 1), std::max<size_t>(1, n / std::max<size_t>(1, min_part)));
+        if(parts <= 1 || W_.empty())
+        {
+            f(0, n);
+            return;
+        }
+        std::lock_guard<std::mutex> run_g(run_mu_);
+        {
+            std::lock_guard<std::mutex> g(mu_);
+            job_ = &f, n_ = n, parts_ = parts, finished_ = 0, next_ = 0;
+            gen_++;
+        }
+        cv_.notify_all();
+        work_parts();
+        std::unique_lock<std::mutex> g(mu_);
+        done_cv_.wait(g, [&](){ return finished_ == parts_; });
+    }
+};
+
+inline void parallel_for(const size_t n, const size_t min_per_thread, const std::function<void(size_t, size_t)>& f)
+{
+    Host_Pool::get().run(n, min_per_thread, f);
 }
 
 inline bool host_acgt(const char c)
@@ -214,6 +289,7 @@ class Engine final : public kache_table
 
     // The table.
     Dev_Buf cs_, spill_, slots_, ov_, ctr_;
+    Dev_Buf cs2_, spill2_, slots2_, ov2_;   // The previous table's arrays, kept for the next resize to build into.
     Dev_Table T_{};
     uint64_t ov_slots_ = 0;
 
@@ -224,7 +300,8 @@ class Engine final : public kache_table
     uint64_t pending_[KACHE_MAX_USERS] = {};
 
     // Batches.
-    Pinned_Buf pin_, pin_ctr_;
+    Pinned_Buf pin_, pin_ctr_, pin_out_;
+    cudaEvent_t ev_out_[2] = {nullptr, nullptr};
     Dev_Buf dbatch_, dout_, dretry_a_, dretry_b_, dscan_, dtmp_;
 
     // Profiling.
@@ -334,7 +411,7 @@ class Engine final : public kache_table
         if((old_cap << d) != new_cap)
             throw std::logic_error("a resize multiplies the bucket count by a power of 2");
         // The new buckets are written whole by split_kernel: no clearing.
-        Dev_Buf cs, spill, slots, ov;
+        Dev_Buf &cs = cs2_, &spill = spill2_, &slots = slots2_, &ov = ov2_;
         cs.ensure(new_cap * B), spill.ensure(new_cap * 32), slots.ensure(new_cap * B * slot_bytes);
         Dev_Table T2{};
         bind(T2, cs, spill, slots, new_cap);
@@ -354,7 +431,7 @@ class Engine final : public kache_table
         check(cudaMemsetAsync(retried, 0, 4, stream_), "memset");
         check(cudaMemsetAsync(dretry_b_.p, 0, total / 8 + 8, stream_), "memset");
         launch(K_RESIZE, [&](){ split_kernel<k, l, set_><<<grid_for(old_cap, 8), 256, 0, stream_>>>(T_, T2, d, dretry_a_.as<unsigned int>()); });
-        launch(K_RESIZE, [&](){ rehash_kernel<k, l, set_><<<grid_for(total / 32 + 1, 8), 256, 0, stream_>>>(T_, T2, dretry_a_.as<unsigned int>(), dretry_b_.as<unsigned int>(), retried); });
+        launch(K_RESIZE, [&](){ rest_kernel<k, l, set_><<<grid_for(total / 1024 + 1, 8), 256, 0, stream_>>>(T_, T2, dretry_a_.as<unsigned int>(), total, dretry_b_.as<unsigned int>(), retried); });
         std::swap(dretry_a_.p, dretry_b_.p), std::swap(dretry_a_.bytes, dretry_b_.bytes);
         while(static_cast<uint32_t>(read_ctr(3)[2]))
         {
@@ -373,7 +450,7 @@ class Engine final : public kache_table
             recount_overflow(T2, ov_slots);
             check(cudaMemsetAsync(dretry_b_.p, 0, total / 8 + 8, stream_), "memset");
             check(cudaMemsetAsync(retried, 0, 4, stream_), "memset");
-            launch(K_RESIZE, [&](){ rehash_kernel<k, l, set_><<<grid_for(total / 32 + 1, 8), 256, 0, stream_>>>(T_, T2, dretry_a_.as<unsigned int>(), dretry_b_.as<unsigned int>(), retried); });
+            launch(K_RESIZE, [&](){ rest_kernel<k, l, set_><<<grid_for(total / 1024 + 1, 8), 256, 0, stream_>>>(T_, T2, dretry_a_.as<unsigned int>(), total, dretry_b_.as<unsigned int>(), retried); });
             std::swap(dretry_a_.p, dretry_b_.p), std::swap(dretry_a_.bytes, dretry_b_.bytes);
         }
         sync();
@@ -405,8 +482,8 @@ class Engine final : public kache_table
 
     // ---- Batches ----
 
-    // Stages a host batch: offsets, positions and segments computed here, bases gathered into pinned memory, one
-    // H2D copy.
+    // Stages a host batch: offsets, positions and segments computed here, bases gathered into pinned memory and copied
+    // in pieces, each piece's H2D copy running while the next one is gathered.
     Batch_Info stage_host(const char* const* seqs, const size_t* lens, const size_t n)
     {
         uint64_t bytes = 0, nsegs = 0, pos = 0;
@@ -451,15 +528,24 @@ class Engine final : public kache_table
                 segs[seg_hist_[len]++] = (uint64_t(i) << 24) | s;
             }
         }
-        parallel_for(n, 4096, [&](const size_t s, const size_t e)
-        {
-            for(size_t i = s; i < e; ++i)
-                if(lens[i])
-                    std::memcpy(bases + off[i], seqs[i], lens[i]);
-        });
         dbatch_.ensure(total);
-        check(cudaMemcpyAsync(dbatch_.p, pin_.p, total, cudaMemcpyHostToDevice, stream_), "H2D batch");
         char* d = dbatch_.as<char>();
+        check(cudaMemcpyAsync(d, pin_.p, o_bases, cudaMemcpyHostToDevice, stream_), "H2D batch");
+        constexpr uint64_t piece = uint64_t(32) << 20;
+        for(size_t i0 = 0; i0 < n; )
+        {
+            size_t i1 = i0;
+            while(i1 < n && off[i1] - off[i0] < piece)
+                i1++;
+            parallel_for(i1 - i0, 2048, [&](const size_t s, const size_t e)
+            {
+                for(size_t i = i0 + s; i < i0 + e; ++i)
+                    if(lens[i])
+                        std::memcpy(bases + off[i], seqs[i], lens[i]);
+            });
+            check(cudaMemcpyAsync(d + o_bases + off[i0], bases + off[i0], off[i1] - off[i0], cudaMemcpyHostToDevice, stream_), "H2D batch");
+            i0 = i1;
+        }
         Batch_Info bi;
         bi.b = Dev_Batch{reinterpret_cast<const uint8_t*>(d + o_bases), reinterpret_cast<const uint64_t*>(d + o_off),
                          reinterpret_cast<const uint64_t*>(d + o_seg), reinterpret_cast<const uint64_t*>(d + o_pos), n, nsegs};
@@ -490,7 +576,6 @@ class Engine final : public kache_table
             check(cub::DeviceScan::InclusiveSum(dscan_.p, tmp, npos, pos_off + 1, static_cast<int64_t>(n), stream_), "scan");
             check(cub::DeviceScan::InclusiveSum(dscan_.p, tmp, nseg, seg_off + 1, static_cast<int64_t>(n), stream_), "scan");
         }
-        pin_ctr_.ensure(64);
         uint64_t* h = pin_ctr_.as<uint64_t>(32);
         check(cudaMemcpyAsync(h, pos_off + n, 8, cudaMemcpyDeviceToHost, stream_), "D2H");
         check(cudaMemcpyAsync(h + 1, seg_off + n, 8, cudaMemcpyDeviceToHost, stream_), "D2H");
@@ -518,7 +603,7 @@ class Engine final : public kache_table
             launch(kind, [&](){ stream_kernel<k, l, Vis><<<grid_for(se - sb, stream_warps), 32 * stream_warps, 0, stream_>>>(bi.b, sb, se, vis); });
             return;
         }
-        const uint64_t blocks = std::min<uint64_t>((se - sb + lane_block - 1) / lane_block, uint64_t(sm_count_) * 8);
+        const uint64_t blocks = std::min<uint64_t>((se - sb + lane_block - 1) / lane_block, uint64_t(sm_count_) * 16);
         launch(kind, [&](){ lane_kernel<k, l, Vis><<<static_cast<unsigned>(blocks), lane_block, 0, stream_>>>(bi.b, sb, se, vis); });
     }
 
@@ -565,7 +650,8 @@ class Engine final : public kache_table
         const uint64_t nsegs = bi.b.nsegs;
         const double pos_per_seg = nsegs ? static_cast<double>(bi.total_pos) / nsegs : 1.0;
         uint64_t total_ins = 0;
-        double novelty = 1.0;
+        // Keys inserted per position: assumed 1/2 for the first chunk, then as the last chunk measured.
+        double novelty = 0.5;
         const size_t bits = bi.total_pos / 8 + 8;
         unsigned int* retried = reinterpret_cast<unsigned int*>(ctr() + 2);
 
@@ -577,11 +663,13 @@ class Engine final : public kache_table
                 check(cudaMemsetAsync(dretry_a_.p, 0, dretry_a_.bytes, stream_), "memset");
                 dretry_dirty_ = false;
             }
+            // A chunk may take the table to 95 % of its slots; the schedule then resizes it, as the reference would.
             const double slots = static_cast<double>(cap_ * B);
-            const double room = std::max(0.0, static_cast<double>(resize_th_) - static_cast<double>(size_)) + 0.1 * slots;
+            const double room = std::max(0.95 * slots - static_cast<double>(size_), 0.05 * slots);
             const double want_pos = room / std::max(novelty, 1e-3);
             uint64_t se = sb + std::max<uint64_t>(1, static_cast<uint64_t>(want_pos / pos_per_seg));
-            se = std::min(se, nsegs);
+            if(se + (se - sb) / 2 >= nsegs)
+                se = nsegs;     // No small last chunk: it would run with too few lanes to fill the GPU.
 
             check(cudaMemsetAsync(ctr(), 0, 8, stream_), "memset");
             check(cudaMemsetAsync(retried, 0, 4, stream_), "memset");
@@ -644,20 +732,33 @@ class Engine final : public kache_table
     }
 
     // Copies device output to a host buffer through pinned memory, in pieces, the copy-out overlapping the next D2H.
+    // Copies device output to a host buffer through two pinned pieces: piece i's D2H copy runs while piece i - 1
+    // is copied out to the caller's buffer by the host pool.
     void d2h(void* dst, const void* src, const size_t bytes)
     {
         if(bytes == 0)
             return;
-        const size_t piece = size_t(64) << 20;
-        pin_.ensure(std::min(bytes, 2 * piece));
-        char* stage[2] = {pin_.as<char>(0), pin_.as<char>(std::min(bytes, piece))};
-        for(size_t o = 0, i = 0; o < bytes; o += piece, ++i)
+        constexpr size_t piece = size_t(32) << 20;
+        pin_out_.ensure(2 * piece);
+        if(!ev_out_[0])
+            check(cudaEventCreateWithFlags(&ev_out_[0], cudaEventDisableTiming), "event"), check(cudaEventCreateWithFlags(&ev_out_[1], cudaEventDisableTiming), "event");
+        char* stage[2] = {pin_out_.as<char>(0), pin_out_.as<char>(piece)};
+        const size_t pieces = (bytes + piece - 1) / piece;
+        const auto copy_out = [&](const size_t i)
         {
-            const size_t m = std::min(piece, bytes - o);
+            const size_t o = i * piece, m = std::min(piece, bytes - o);
+            check(cudaEventSynchronize(ev_out_[i & 1]), "event sync");
+            parallel_for(m, size_t(2) << 20, [&](const size_t s, const size_t e){ std::memcpy(static_cast<char*>(dst) + o + s, stage[i & 1] + s, e - s); });
+        };
+        for(size_t i = 0; i < pieces; ++i)
+        {
+            const size_t o = i * piece, m = std::min(piece, bytes - o);
             check(cudaMemcpyAsync(stage[i & 1], static_cast<const char*>(src) + o, m, cudaMemcpyDeviceToHost, stream_), "D2H");
-            sync();
-            parallel_for(m, size_t(4) << 20, [&](const size_t s, const size_t e){ std::memcpy(static_cast<char*>(dst) + o + s, stage[i & 1] + s, e - s); });
+            check(cudaEventRecord(ev_out_[i & 1], stream_), "event record");
+            if(i > 0)
+                copy_out(i - 1);
         }
+        copy_out(pieces - 1);
     }
 
     static Op_Fn<VT> op_fn(const uint32_t op, const uint64_t x, const uint64_t init) { return Op_Fn<VT>{op, static_cast<VT>(x), static_cast<VT>(init)}; }
@@ -696,6 +797,9 @@ public:
             cudaStreamSynchronize(stream_);
         for(auto& e : ev_)
             cudaEventDestroy(e.a), cudaEventDestroy(e.b);
+        for(auto& e : ev_out_)
+            if(e)
+                cudaEventDestroy(e);
         if(own_)
             cudaStreamDestroy(own_);
     }
@@ -775,7 +879,7 @@ public:
         auto* dk = dout_.as<uint64_t>();
         auto* dh = dk + P;
         auto* dc = reinterpret_cast<uint8_t*>(dh + P);
-        stream_launch(K_OTHER, bi, 0, bi.b.nsegs, Describe_Visitor{bi.b.pos_off, dk, dh, dc, dc + P, dc + 2 * P}, true);
+        stream_launch(K_OTHER, bi, 0, bi.b.nsegs, Describe_Visitor{bi.b.pos_off, dk, dh, dc, dc + P, dc + 2 * P, false}, true);
         d2h(key, dk, P * 8), d2h(h, dh, P * 8), d2h(cs, dc, P), d2h(fwd, dc + P, P), d2h(valid, dc + 2 * P, P);
     }
 

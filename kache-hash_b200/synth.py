@@ -92,11 +92,78 @@ def reads_variable(g, coverage, median, sigma, lo, hi, seed, rc=0.5, sub=0.005, 
     return _pack(reads)
 
 
+def reads_lognormal(g, coverage, median, sigma, lo, hi, seed, rc=0.5, sub=0.005, n_rate=0.0005, chunk=1 << 24):
+    """Vectorised reads of log-normal lengths clipped to [lo, hi], to `coverage` x of g, with substitutions and N's
+    (no indels): as (bases, offsets)."""
+    rng = np.random.default_rng(seed)
+    total = int(len(g) * coverage)
+    est = int(total / (median * np.exp(sigma * sigma / 2))) + 16
+    lens = np.clip(rng.lognormal(np.log(median), sigma, size=est * 2), lo, hi).astype(np.int64)
+    cut = int(np.searchsorted(np.cumsum(lens), total)) + 1
+    lens = np.minimum(lens[:cut], len(g))
+    n = len(lens)
+    starts = (rng.random(n) * (len(g) - lens + 1)).astype(np.int64)
+    flip = rng.random(n) < rc
+    off = np.zeros(n + 1, np.uint64)
+    np.cumsum(lens, out=off[1:])
+    out = np.empty(int(off[-1]) + 16, np.uint8)
+    out[-16:] = 0
+    # Read i's base j comes from first[i] + j * step[i]: forward from its start, or backward from its end.
+    first = starts + np.where(flip, lens - 1, 0)
+    step = np.where(flip, -1, 1).astype(np.int64)
+    xor = np.where(flip, 3, 0).astype(np.uint8)
+    offi = off.astype(np.int64)
+    b = 0
+    while b < n:
+        e = min(n, int(np.searchsorted(off, off[b] + chunk, side="right")))
+        e = max(e, b + 1)
+        L = lens[b:e]
+        rid = np.repeat(np.arange(b, e), L)
+        j = np.arange(offi[b], offi[e], dtype=np.int64)
+        j -= offi[rid]
+        j *= step[rid]
+        j += first[rid]
+        r = g[j]
+        r ^= xor[rid]
+        u = rng.integers(0, 1 << 16, size=len(r), dtype=np.uint16)
+        if sub > 0:
+            m = np.flatnonzero(u < int(sub * 65536))
+            r[m] = (r[m] + rng.integers(1, 4, size=len(m), dtype=np.uint8)) % 4
+        if n_rate > 0:
+            r[(u >= 65535 - int(n_rate * 65536))] = 4
+        out[int(off[b]):int(off[e])] = ASCII[r]
+        b = e
+    return out, off
+
+
 def stretches(g, length):
     """The genome as pieces of `length` bases (the last one shorter), as (bases, offsets): a 1x streaming of it."""
     n = (len(g) + length - 1) // length
     off = np.minimum(np.arange(n + 1, dtype=np.uint64) * np.uint64(length), np.uint64(len(g)))
     return np.concatenate([ASCII[g], np.zeros(16, np.uint8)]), off
+
+
+# The counter workload: a 100 Mbp genome, 5 % of it segmental duplications of 1-20 kb at 2 % divergence, primed
+# with its 31-mers; counted from 30x reads of log-normal lengths (median 150, sigma 0.6) clipped to 50-1000 bp.
+def config2(scale=1.0):
+    g = genome(int(100_000_000 * scale), seed=21, dup_frac=0.05, dup_len=(1000, 20000), dup_div=0.02)
+    index = stretches(g, 1_000_000)
+    reads = reads_lognormal(g, 30, 150, 0.6, 50, 1000, seed=22)
+    return g, index, reads
+
+
+# The oriented workload: a 50 Mbp genome, reads of log-normal lengths (median 10 kb, sigma 0.8) clipped to 1-100 kb at
+# 5x, 5 % errors split 3:1:1 substitution:insertion:deletion, half reverse-complemented.
+def config3(scale=1.0):
+    g = genome(int(50_000_000 * scale), seed=31)
+    reads = reads_variable(g, 5, 10_000, 0.8, 1000, 100_000, seed=32, rc=0.5, sub=0.03, ins=0.01, dele=0.01)
+    return g, reads
+
+
+# The resize-heavy set: a 400 Mbp genome streamed as 150 bp pieces at 1x into a set sized for 1M keys.
+def config4(scale=1.0):
+    g = genome(int(400_000_000 * scale), seed=41)
+    return g, stretches(g, 150)
 
 
 # The benchmark workload of the headline metric: a map <31, u64, 22> sized for 10M keys; upsert(c + 1, init 1) of

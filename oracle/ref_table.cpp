@@ -293,6 +293,50 @@ double ref_bench_upsert(void* tv, const char* bases, const uint64_t* off, uint64
     return now_s() - t0;
 }
 
+// As ref_bench_upsert, for upsert_oriented (op, x_fwd, x_rev) and for present-only updates (op, x).
+double ref_bench_upsert_oriented(void* tv, const char* bases, const uint64_t* off, uint64_t n, uint32_t batch, uint32_t threads, uint32_t op, uint64_t xf, uint64_t xr, uint64_t* out)
+{
+    auto* t = static_cast<Table*>(tv);
+    std::vector<uint32_t> users(threads);
+    for(auto& u : users)
+        u = t->reg();
+    std::atomic<uint64_t> next{0}, total{0};
+    const double t0 = now_s();
+    std::vector<std::thread> W;
+    for(uint32_t w = 0; w < threads; ++w)
+        W.emplace_back([&, w]()
+        {
+            uint64_t c = 0;
+            for(uint64_t b; (b = next++) * batch < n; )
+                c += t->upsert_oriented(users[w], Batch(bases, off, n, b * batch, (b + 1) * batch), op, xf, xr);
+            total += c;
+        });
+    for(auto& w : W)
+        w.join();
+    *out = total;
+    return now_s() - t0;
+}
+
+double ref_bench_update(void* tv, const char* bases, const uint64_t* off, uint64_t n, uint32_t batch, uint32_t threads, uint32_t op, uint64_t x, uint64_t* out)
+{
+    auto* t = static_cast<Table*>(tv);
+    std::atomic<uint64_t> next{0}, total{0};
+    const double t0 = now_s();
+    std::vector<std::thread> W;
+    for(uint32_t w = 0; w < threads; ++w)
+        W.emplace_back([&]()
+        {
+            uint64_t c = 0;
+            for(uint64_t b; (b = next++) * batch < n; )
+                c += t->update(Batch(bases, off, n, b * batch, (b + 1) * batch), op, x);
+            total += c;
+        });
+    for(auto& w : W)
+        w.join();
+    *out = total;
+    return now_s() - t0;
+}
+
 double ref_bench_count(void* tv, const char* bases, const uint64_t* off, uint64_t n, uint32_t batch, uint32_t threads, uint64_t* out)
 {
     auto* t = static_cast<Table*>(tv);

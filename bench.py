@@ -16,7 +16,6 @@ workload with all host threads.
 import argparse
 import json
 import os
-import subprocess
 import sys
 import threading
 import time
@@ -42,43 +41,56 @@ def load_peaks():
 
 
 class Clocks:
-    """nvidia-smi samples during the timed region."""
+    """SM clock and clock-event reasons sampled through NVML (read-only queries) every 10 ms during the timed region,
+    from a thread of this process: the library is initialised before the region starts, so nothing starts up inside
+    it. Reports "unavailable" without NVML."""
 
-    def __init__(self, gpu_index):
-        self.rows, self.proc = [], None
-        self.gpu = gpu_index
+    NAMES = [("hw_slowdown", "nvmlClocksEventReasonHwSlowdown"), ("hw_thermal_slowdown", "nvmlClocksEventReasonHwThermalSlowdown"),
+             ("sw_thermal_slowdown", "nvmlClocksEventReasonSwThermalSlowdown"), ("sw_power_cap", "nvmlClocksEventReasonSwPowerCap")]
+
+    def __init__(self, device):
+        import torch
+        self.rows, self.h, self.run = [], None, False
+        try:
+            import pynvml
+            pynvml.nvmlInit()
+            self.nv = pynvml
+            try:
+                self.h = pynvml.nvmlDeviceGetHandleByUUID("GPU-" + str(torch.cuda.get_device_properties(device).uuid))
+            except Exception:
+                self.h = pynvml.nvmlDeviceGetHandleByIndex(device)
+            self.max_mhz = pynvml.nvmlDeviceGetMaxClockInfo(self.h, pynvml.NVML_CLOCK_SM)
+        except Exception:
+            self.h = None
+
+    def _sample(self):
+        nv = self.nv
+        while self.run:
+            try:
+                self.rows.append((nv.nvmlDeviceGetClockInfo(self.h, nv.NVML_CLOCK_SM),
+                                  nv.nvmlDeviceGetCurrentClocksEventReasons(self.h)))
+            except Exception:
+                pass
+            time.sleep(0.01)
 
     def start(self):
-        q = "clocks.sm,clocks.max.sm,utilization.gpu,clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap"
-        try:
-            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={q}", "--format=csv,noheader,nounits", "-lms", "100"],
-                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
-            self.t = threading.Thread(target=self._read, daemon=True)
-            self.t.start()
-        except OSError:
-            self.proc = None
-
-    def _read(self):
-        for line in self.proc.stdout:
-            self.rows.append([x.strip() for x in line.split(",")])
+        if self.h is None:
+            return
+        self.run = True
+        self.t = threading.Thread(target=self._sample, daemon=True)
+        self.t.start()
 
     def stop(self):
-        if self.proc is None:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
-        self.proc.terminate()
-        try:
-            self.proc.wait(timeout=5)
-        except subprocess.TimeoutExpired:
-            self.proc.kill()
-        rows = [r for r in self.rows if len(r) >= 7]
-        busy = [r for r in rows if r[2].isdigit() and int(r[2]) > 0] or rows
-        if not busy:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
-        sm = sorted(int(r[0]) for r in busy if r[0].isdigit())
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[i] for r in busy for i in range(4) if r[3 + i].lower() == "active"})
-        return {"sm_mhz": sm[len(sm) // 2] if sm else None, "sm_max_mhz": int(busy[0][1]) if busy[0][1].isdigit() else None,
-                "reasons": reasons, "samples": len(busy)}
+        if self.h is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvml unavailable"]}
+        self.run = False
+        self.t.join()
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": self.max_mhz, "reasons": ["no samples"]}
+        sm = sorted(r[0] for r in self.rows)
+        reasons = sorted({name for _, mask in self.rows for name, const in self.NAMES if mask & getattr(self.nv, const)})
+        return {"sm_mhz": sm[len(sm) // 2], "sm_max_mhz": self.max_mhz, "reasons": reasons, "samples": len(self.rows),
+                "source": "nvml, 10 ms"}
 
 
 def dist_env():
@@ -120,7 +132,7 @@ def positions(off, k=31):
 
 def cpu_baseline_sample(ins, held, threads):
     """The reference's own table (oracle/_ref) on a bounded sample of the same workload: a tenth of the upsert reads
-    into a table sized for a tenth of the keys, then counts over a tenth of the held-out reads."""
+    into a table sized for a tenth of the keys, then per-position finds over a tenth of the held-out reads."""
     import oracle
     L = oracle.ref()
     if L is None:
@@ -131,11 +143,24 @@ def cpu_baseline_sample(ins, held, threads):
     t = L.ref_new(0, N_KEYS // 10, 0.8, 0, threads)
     out = oracle._u64()
     t_up = L.ref_bench_upsert(t, si.bases.ctypes.data, si.off.ctypes.data, si.n, 64, threads, 16, 1, oracle.ctypes.byref(out))
-    t_q = L.ref_bench_count(t, sh.bases.ctypes.data, sh.off.ctypes.data, sh.n, 64, threads, oracle.ctypes.byref(out))
+    t_q = ref_lookup_timed(L, t, sh, threads)
     L.ref_free(t)
     p = positions(si.off) + positions(sh.off)
     return {"value": p / (t_up + t_q), "unit": "k-mers/s", "cores": threads, "kind": "reference",
-            "sample": f"upsert {si.n} reads + count {sh.n} held-out reads ({p} positions), batches of 64 reads, {threads} threads"}
+            "sample": f"upsert {si.n} reads + per-position find over {sh.n} held-out reads ({p} positions), batches of 64 reads, {threads} threads"}
+
+
+def ref_lookup_timed(L, t, b, threads):
+    """Seconds for the reference's per-position find over batch b (found flags and values into host arrays, as
+    kache_lookup returns them)."""
+    lens = np.diff(b.off).astype(np.int64)
+    pos_off = np.zeros(b.n + 1, np.uint64)
+    np.cumsum(np.maximum(lens - 30, 0), out=pos_off[1:])
+    P = int(pos_off[-1])
+    found = np.zeros(max(P, 1), np.uint8)
+    vals = np.zeros(max(P, 1), np.uint64)
+    return L.ref_bench_lookup(t, b.bases.ctypes.data, b.off.ctypes.data, b.n, pos_off.ctypes.data, 64, threads,
+                              found.ctypes.data, vals.ctypes.data)
 
 
 def run_reference(args):
@@ -157,7 +182,7 @@ def run_reference(args):
     for s in range(args.warmup + args.steps):
         t = L.ref_new(0, N_KEYS, 0.8, 0, threads)
         t_up = L.ref_bench_upsert(t, bi.bases.ctypes.data, bi.off.ctypes.data, bi.n, 64, threads, 16, 1, oracle.ctypes.byref(out))
-        t_q = L.ref_bench_count(t, bh.bases.ctypes.data, bh.off.ctypes.data, bh.n, 64, threads, oracle.ctypes.byref(out))
+        t_q = ref_lookup_timed(L, t, bh, threads)
         L.ref_free(t)
         if s >= args.warmup:
             times.append(t_up + t_q)
@@ -167,9 +192,9 @@ def run_reference(args):
                       "warmup": args.warmup, "ms_per_step": 1000 * T / args.steps, "higher_is_better": True, "scaling": "weak",
                       "vs_baseline": None, "dtype": "u64", "data": "synthetic",
                       "config": {"workload": "config 1: <31,u64,22> n=10M; upsert(c+1, init 1) 333,333 x 150 bp; find 1M x 150 bp held-out",
-                                 "upsert_positions": positions(bi.off), "find_positions": positions(bh.off), "find": "count per read"},
+                                 "upsert_positions": positions(bi.off), "find_positions": positions(bh.off), "find": "per-position found flag and value"},
                       "cpu_baseline": {"value": v, "unit": "k-mers/s", "cores": threads, "kind": "reference",
-                                       "sample": "the whole workload per step, batches of 64 reads round-robin over the threads"},
+                                       "sample": "the whole workload per step (upsert, then per-position find), batches of 64 reads round-robin over the threads"},
                       "e2e": {"value": v, "unit": "k-mers/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}))
 
 
@@ -208,13 +233,38 @@ def run_b200(args):
         T.upsert_dev(u, d_ins_b.data_ptr(), d_ins_o.data_ptr(), bi.n, kache.ADD_WRAP, 1, 1)
         T.lookup_dev(d_held_b.data_ptr(), d_held_o.data_ptr(), bh.n, d_found.data_ptr(), d_vals.data_ptr(), None)
 
-    found_h = np.empty(P_find, np.uint8)
-    vals_h = np.empty(P_find, np.uint64)
+    # End-to-end buffers: the reads and the lookup outputs in page-locked host memory, which the library copies
+    # to and from directly.
+    def pinned(a):
+        t = torch.empty(a.nbytes, dtype=torch.uint8, pin_memory=True)
+        v = t.numpy().view(a.dtype)
+        v[:] = a
+        return t, v
 
-    def step_e2e():
+    keep = []
+    def pinned_batch(b):
+        t, v = pinned(b.bases)
+        keep.append(t)
+        return Batch(v, b.off)
+
+    pi, ph = pinned_batch(bi), pinned_batch(bh)
+    t_f, found_h = pinned(np.zeros(P_find, np.uint8))
+    t_v, vals_h = pinned(np.zeros(P_find, np.uint64))
+    found_pg, vals_pg = np.zeros(P_find, np.uint8), np.zeros(P_find, np.uint64)
+
+    e2e_parts = {"clear": 0.0, "insert": 0.0, "lookup": 0.0}
+
+    def step_e2e(ins=pi, held=ph, found=found_h, vals=vals_h):
+        t0 = time.perf_counter()
         T.clear()
-        kache.lib().kache_insert(T.h, u, *bi.args(), kache.ADD, 1, None)
-        kache.lib().kache_lookup(T.h, *bh.args(), found_h.ctypes.data, vals_h.ctypes.data, None)
+        t1 = time.perf_counter()
+        kache.lib().kache_insert(T.h, u, *ins.args(), kache.ADD, 1, None)
+        t2 = time.perf_counter()
+        kache.lib().kache_lookup(T.h, *held.args(), found.ctypes.data, vals.ctypes.data, None)
+        t3 = time.perf_counter()
+        e2e_parts["clear"] += t1 - t0
+        e2e_parts["insert"] += t2 - t1
+        e2e_parts["lookup"] += t3 - t2
 
     def barrier():
         torch.cuda.synchronize()
@@ -226,10 +276,9 @@ def run_b200(args):
     for _ in range(args.warmup):
         step_dev()
     barrier()
-    clocks = Clocks(local)
-    if not args.only_dev:
+    clocks = Clocks(local) if not args.only_dev else None
+    if clocks is not None:
         clocks.start()
-        time.sleep(0.3)
     launches0 = kache.kernel_launches()
     T.profile(True)
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -242,7 +291,7 @@ def run_b200(args):
     launches = kache.kernel_launches() - launches0
     prof = {kind: T.profile_read(i) for i, kind in enumerate(["upsert", "update", "lookup", "reduce", "resize", "other"])}
     T.profile(False)
-    clk = clocks.stop() if not args.only_dev else None
+    clk = clocks.stop() if clocks is not None else None
 
     # Per-kernel roofline: algorithmic bytes per launch over the kernel's mean event-timed duration.
     st = T.stats()
@@ -269,16 +318,30 @@ def run_b200(args):
     d = kernels[dom]
 
     # End to end through the C interface with host buffers.
-    e2e_ms = float("nan")
+    e2e_ms = e2e_pg_ms = float("nan")
+    parts_pinned, pg_steps = {}, 0
     if not args.only_dev:
         for _ in range(max(1, args.warmup // 2)):
             step_e2e()
         barrier()
+        for key_ in e2e_parts:
+            e2e_parts[key_] = 0.0
         t0 = time.perf_counter()
         for _ in range(args.steps):
             step_e2e()
         barrier()
         e2e_ms = max_over_ranks(dist, (time.perf_counter() - t0) * 1000, dev) / args.steps
+        parts_pinned = {key_: 1000 * v_ / args.steps for key_, v_ in e2e_parts.items()}
+        # The same calls with pageable host buffers (a few steps): the library stages them through its own pinned
+        # memory.
+        pg_steps = max(1, min(args.steps, 5))
+        step_e2e(bi, bh, found_pg, vals_pg)
+        barrier()
+        t0 = time.perf_counter()
+        for _ in range(pg_steps):
+            step_e2e(bi, bh, found_pg, vals_pg)
+        barrier()
+        e2e_pg_ms = max_over_ranks(dist, (time.perf_counter() - t0) * 1000, dev) / pg_steps
 
     if rank == 0:
         line = {
@@ -296,7 +359,9 @@ def run_b200(args):
                          "model": "A = b_in + b_out + 32*rho + 32*r_slot + 32*w_slot bytes per k-mer; rho from the describer on 5000 reads"},
             "e2e": {"value": P * ws / (e2e_ms * 1e-3), "unit": "k-mers/s", "ms_per_step": e2e_ms,
                     "h2d_bytes_per_step": int(bi.off[-1] + bh.off[-1] + 16 * (bi.n + bh.n)),
-                    "d2h_bytes_per_step": int(P_find * 9)},
+                    "d2h_bytes_per_step": int(P_find * 9),
+                    "host_buffers": "page-locked (reads and outputs)", "ms_per_call": parts_pinned,
+                    "pageable": {"value": P * ws / (e2e_pg_ms * 1e-3), "ms_per_step": e2e_pg_ms, "steps": pg_steps}},
             "clocks": clk,
         }
         cb = None if args.only_dev else cpu_baseline_sample(ins, held, min(128, os.cpu_count() or 1))
@@ -327,8 +392,8 @@ def run_density(kache, b):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=10)
-    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--steps", type=int, default=30)
+    ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--only-dev", action="store_true",
                     help="time the device-resident steps only (no e2e, CPU baseline or clock sampling): the profiling case")

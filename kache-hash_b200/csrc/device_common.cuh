@@ -23,6 +23,8 @@ constexpr int B = 32;                  // Slots per bucket: a bucket's 32 checks
 constexpr uint64_t max_buckets = (uint64_t(1) << 32) - 1;
 constexpr int seg_rows = 16;           // Rows of 32 k-mer positions that one warp describes in a segment.
 constexpr int seg_positions = 32 * seg_rows;
+constexpr int lane_seg_positions = 64; // Positions of a lane's segment: short, so that a batch has many lanes.
+constexpr uint64_t max_seg_index = 0xFFFFFF;   // Segment indexes take 24 bits of a segment list entry.
 
 enum Op : uint32_t { OP_KEEP = 0, OP_ASSIGN = 1, OP_ADD = 2, OP_OR = 3, OP_MIN = 4, OP_MAX = 5, OP_ADD_WRAP = 16 };
 
@@ -49,6 +51,8 @@ __host__ __device__ __forceinline__ uint8_t checksum_of(const uint64_t key)
     const uint8_t c = static_cast<uint8_t>((key * 0x9E3779B97F4A7C15ull) >> 56);
     return c ? c : 1;
 }
+
+__device__ __forceinline__ uint64_t min64(const uint64_t a, const uint64_t b) { return a < b ? a : b; }
 
 __host__ __device__ __forceinline__ uint64_t kmer_mask(const int k) { return k == 32 ? ~0ull : (1ull << (2 * k)) - 1; }
 
@@ -113,18 +117,6 @@ __device__ __forceinline__ uint64_t minimizer_hash(const uint64_t key)
     return h;
 }
 
-// Spreads the 32 bits of x to the even bits of a 64-bit word.
-__device__ __forceinline__ uint64_t spread32(const uint32_t x)
-{
-    uint64_t v = x;
-    v = (v | (v << 16)) & 0x0000FFFF0000FFFFull;
-    v = (v | (v << 8)) & 0x00FF00FF00FF00FFull;
-    v = (v | (v << 4)) & 0x0F0F0F0F0F0F0F0Full;
-    v = (v | (v << 2)) & 0x3333333333333333ull;
-    v = (v | (v << 1)) & 0x5555555555555555ull;
-    return v;
-}
-
 // Bit 7 of each byte of the result is set iff that byte of w is zero, exactly (no carries cross bytes).
 __device__ __forceinline__ uint32_t zero_bytes(const uint32_t w)
 {
@@ -136,6 +128,28 @@ __device__ __forceinline__ uint32_t gather4(const uint32_t y)
 {
     return (((y >> 7) * 0x00204081u) >> 21) & 0xFu;
 }
+
+// The slots of a bucket whose checksum byte (of the 32 bytes a, b) may equal c, as bit 8q + i for byte q of word i,
+// that is slot 4i + q (`candidate_slot`): a spread cheaper than slot order. With exact_, exactly the bytes equal to
+// c. Without, every byte equal to c and possibly the byte just above one in the same word (the borrow of the
+// subtraction reaches it only if it equals c ^ 1): callers verify candidates by their keys.
+template <bool exact_>
+__device__ __forceinline__ uint32_t candidates32(const uint4 a, const uint4 b, const uint32_t c)
+{
+    const uint32_t cc = c * 0x01010101u;
+    const uint32_t w[8] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w};
+    uint32_t m = 0;
+#pragma unroll
+    for(int i = 0; i < 8; ++i)
+    {
+        const uint32_t t = w[i] ^ cc;
+        const uint32_t y = exact_ ? zero_bytes(t) : (t - 0x01010101u) & ~t & 0x80808080u;
+        m |= y >> (7 - i);
+    }
+    return m;
+}
+
+__device__ __forceinline__ uint32_t candidate_slot(const uint32_t bit) { return 4 * (bit & 7) + (bit >> 3); }
 
 // Bit j of the result is set iff byte j of the 32 bytes (a, b) equals c.
 __device__ __forceinline__ uint32_t match32(const uint4 a, const uint4 b, const uint32_t c)

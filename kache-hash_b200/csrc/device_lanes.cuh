@@ -20,8 +20,6 @@ namespace kache_b200
 
 constexpr int lane_block = 256;     // Threads per block of the lane kernel.
 
-__device__ __forceinline__ uint64_t min64(const uint64_t a, const uint64_t b) { return a < b ? a : b; }
-
 template <int k, int l, typename Visitor>
 __global__ void __launch_bounds__(lane_block) lane_kernel(const Dev_Batch batch, const uint64_t seg_b, const uint64_t seg_e, Visitor vis)
 {
@@ -46,9 +44,9 @@ __global__ void __launch_bounds__(lane_block) lane_kernel(const Dev_Batch batch,
             const uint64_t packed = batch.segs[g];
             q = packed >> 24;
             const uint64_t b0 = batch.off[q], len = batch.off[q + 1] - b0;
-            p0 = (packed & 0xFFFFFF) * seg_positions;
+            p0 = (packed & 0xFFFFFF) * batch.seg_len;
             obase = batch.pos_off[q] + p0;
-            npos = static_cast<uint32_t>(min(len - k + 1 - p0, static_cast<uint64_t>(seg_positions)));
+            npos = static_cast<uint32_t>(min(len - k + 1 - p0, static_cast<uint64_t>(batch.seg_len)));
             p = batch.bases + b0 + p0;
             steps = npos + k - 1;
         }

@@ -296,7 +296,7 @@ __global__ void get_kernel(const Dev_Table T, const uint64_t* keys, const uint64
 }
 
 // Device-side batch preparation, for batches already in HBM: per sequence, its positions and segments.
-static __global__ void batch_counts_kernel(const uint64_t* off, const uint64_t n, const int k, uint64_t* npos, uint64_t* nseg)
+static __global__ void batch_counts_kernel(const uint64_t* off, const uint64_t n, const int k, const uint32_t seg_len, uint64_t* npos, uint64_t* nseg, unsigned int* too_long)
 {
     const uint64_t q = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x;
     if(q >= n)
@@ -304,7 +304,9 @@ static __global__ void batch_counts_kernel(const uint64_t* off, const uint64_t n
     const uint64_t len = off[q + 1] - off[q];
     const uint64_t p = len >= uint64_t(k) ? len - k + 1 : 0;
     npos[q] = p;
-    nseg[q] = (p + seg_positions - 1) / seg_positions;
+    nseg[q] = (p + seg_len - 1) / seg_len;
+    if(nseg[q] > max_seg_index + 1)
+        atomicOr(too_long, 1u);
 }
 
 static __global__ void batch_segs_kernel(const uint64_t* seg_off, const uint64_t n, uint64_t* segs)

@@ -4,11 +4,12 @@
 // What it computes per position is the reference describers' description (include/Kmer_Batch.hpp:191-250,
 // include/Kmer_Lanes.hpp:164-244): the canonical key, its orientation, its checksum and its l-minimizer hash. How:
 //   - each row of 32 bases is loaded coalesced (lane j reads base j), turned into 2-bit codes and an ACGT bit, and
-//     packed with three ballots into a forward word W (first base most significant) and a complemented word R
+//     packed by warp OR-reductions into a forward word W (first base most significant) and a complemented word R
 //     (first base least significant), once per row rather than once per k-mer;
 //   - lane j's k-mer is a 2k-bit funnel window of (W_r, W_r+1) and its reverse complement one of (R_r, R_r+1);
-//   - l-mer hashes of a row go to a per-warp ring in shared memory, and a k-mer's minimizer hash is the least of
-//     the w = k - l + 1 hashes from its own position on;
+//   - each lane hashes the l-mer at its position; the minima of neighbouring pairs of those hashes go to a per-warp
+//     ring in shared memory, and a k-mer's minimizer hash, the least of the w = k - l + 1 hashes from its own position
+//     on, is the least of ceil(w / 2) pair minima;
 //   - non-ACGT characters split sequences (DNA_Utility.hpp:199-224): a window with one is not a k-mer.
 // Sequences are cut into segments of up to `seg_positions` positions; each segment re-reads the k - 1 bases it
 // shares with the next, so segments, like the reference's lanes (include/Streaming_Kmer_Hash_Table.hpp:1751-1781),
@@ -20,8 +21,8 @@
 namespace kache_b200
 {
 
-// A batch on the device: sequence q is bases[off[q], off[q+1]); segs lists (q << 24 | s) for the s'th segment of
-// each sequence of at least k bases; pos_off[q] counts the positions of the sequences before q.
+// A batch on the device: sequence q is bases[off[q], off[q+1]); segs lists (q << 24 | s) for the s'th segment, of
+// seg_len positions, of each sequence of at least k bases; pos_off[q] counts the positions of the sequences before q.
 struct Dev_Batch
 {
     const uint8_t* bases;
@@ -30,6 +31,7 @@ struct Dev_Batch
     const uint64_t* pos_off;
     uint64_t n;
     uint64_t nsegs;
+    uint32_t seg_len;   // A multiple of 32.
 };
 
 constexpr int stream_warps = 8;
@@ -43,19 +45,22 @@ struct Row
 
 __device__ __forceinline__ Row load_row(const uint8_t* seq, const uint64_t len, const uint64_t p, const uint32_t lane)
 {
+    constexpr uint32_t all = 0xFFFFFFFFu;
     const uint64_t pos = p + lane;
     const uint32_t ch = pos < len ? seq[pos] : 0u;
-    const uint32_t x = ch | 0x20u;
-    const bool ok = (x == 'a') | (x == 'c') | (x == 'g') | (x == 't');
+    const uint32_t x = (ch | 0x20u) - 'a';
+    const bool ok = x < 20u && ((0x80045u >> x) & 1u);     // a, c, g, t
     const uint32_t code = ((ch >> 2) ^ (ch >> 1)) & 3u;
-    const uint32_t lo = __ballot_sync(0xFFFFFFFFu, code & 1u);
-    const uint32_t hi = __ballot_sync(0xFFFFFFFFu, code >> 1);
+    const bool first = lane < 16;
+    const uint32_t s = 2 * (lane & 15);
+    const uint32_t f = code << (30 - s), z = code << s;
     Row r;
-    r.valid = __ballot_sync(0xFFFFFFFFu, ok);
-    const uint64_t z = spread32(lo) | (spread32(hi) << 1);   // Base j at bits 2j, 2j+1.
-    uint64_t t = __brevll(z);
-    r.W = ((t >> 1) & 0x5555555555555555ull) | ((t & 0x5555555555555555ull) << 1);  // Base 0 at bits 63..62.
-    r.R = ~z;   // Complemented bases, base j at bits 2j.
+    r.valid = __ballot_sync(all, ok);
+    // Base j at bits 63 - 2j .. 62 - 2j of W, and at bits 2j .. 2j + 1 of ~R.
+    const uint32_t w_hi = __reduce_or_sync(all, first ? f : 0u), w_lo = __reduce_or_sync(all, first ? 0u : f);
+    const uint32_t z_lo = __reduce_or_sync(all, first ? z : 0u), z_hi = __reduce_or_sync(all, first ? 0u : z);
+    r.W = (uint64_t(w_hi) << 32) | w_lo;
+    r.R = ~((uint64_t(z_hi) << 32) | z_lo);
     return r;
 }
 
@@ -96,7 +101,10 @@ template <int k, int l, typename Visitor>
 __global__ void __launch_bounds__(32 * stream_warps) stream_kernel(const Dev_Batch batch, const uint64_t seg_b, const uint64_t seg_e, Visitor vis)
 {
     constexpr int w = k - l + 1;
-    static_assert(k <= 32 && l <= k && w <= 32, "k-mers in a machine word");
+    static_assert(k <= 32 && l < k && w <= 32, "k-mers in a machine word, minimizers of at least two l-mers");
+    constexpr uint32_t all = 0xFFFFFFFFu;
+    // Pair minima: entry 32 (r & 1) + j is min(H[i - 1], H[i]) for position i = 32 r + j of the segment, where H are
+    // the l-mer hashes; rows r and r + 1 are held.
     __shared__ uint64_t ring_all[stream_warps][64];
     const uint32_t lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     uint64_t* ring = ring_all[wid];
@@ -110,16 +118,19 @@ __global__ void __launch_bounds__(32 * stream_warps) stream_kernel(const Dev_Bat
         const uint64_t b0 = batch.off[q], len = batch.off[q + 1] - b0;
         const uint8_t* seq = batch.bases + b0;
         const uint64_t npos = len - k + 1;
-        const uint64_t p0 = s * seg_positions;
-        const uint64_t p1 = min(npos, p0 + seg_positions);
+        const uint64_t p0 = s * batch.seg_len;
+        const uint64_t p1 = min(npos, p0 + batch.seg_len);
         const uint32_t rows = static_cast<uint32_t>((p1 - p0 + 31) / 32);
 
         Row r0 = load_row(seq, len, p0, lane);
         Row r1 = load_row(seq, len, p0 + 32, lane);
+        uint64_t hprev;     // This lane's l-mer hash in the newest row hashed.
         {
             uint64_t f, rc;
             window<l>(r0, r1, lane, f, rc);
-            ring[lane] = wang_u64(f < rc ? f : rc);
+            hprev = wang_u64(f < rc ? f : rc);
+            const uint64_t left = __shfl_up_sync(all, hprev, 1);
+            ring[lane] = lane ? min64(left, hprev) : hprev;  // Entry 0 is never read.
         }
 
         vis.begin_segment(q);
@@ -129,7 +140,10 @@ __global__ void __launch_bounds__(32 * stream_warps) stream_kernel(const Dev_Bat
             {
                 uint64_t f, rc;
                 window<l>(r1, r2, lane, f, rc);
-                ring[((r + 1) & 1) * 32 + lane] = wang_u64(f < rc ? f : rc);
+                const uint64_t hc = wang_u64(f < rc ? f : rc);
+                const uint64_t up = __shfl_up_sync(all, hc, 1), last = __shfl_sync(all, hprev, 31);
+                ring[((r + 1) & 1) * 32 + lane] = min64(lane ? up : last, hc);
+                hprev = hc;
             }
             __syncwarp();
 
@@ -146,14 +160,15 @@ __global__ void __launch_bounds__(32 * stream_warps) stream_kernel(const Dev_Bat
             d.key = f < rc ? f : rc;
             d.fwd = f <= rc;
             d.c = checksum_of(d.key);
+            // Pairs (i - 1, i) at i = j + 1, j + 3, ...: w / 2 of them cover [j, j + w - 1] for even w; for odd w the
+            // pair at j + w - 1 adds the last hash.
             uint64_t h = ~0ull;
             const uint32_t base = (r & 1) * 32 + lane;
 #pragma unroll
-            for(int x = 0; x < w; ++x)
-            {
-                const uint64_t v = ring[(base + x) & 63];
-                h = v < h ? v : h;
-            }
+            for(int o = 1; o < w; o += 2)
+                h = min64(h, ring[(base + o) & 63]);
+            if constexpr(w % 2 == 1)
+                h = min64(h, ring[(base + w - 1) & 63]);
             d.h = h;
 
             vis.visit(d, lane);
@@ -297,15 +312,16 @@ struct Lookup_Visitor
     __device__ __forceinline__ void visit(const Kmer_Desc& d, const uint32_t)
     {
         const unsigned long long* v = nullptr;
+        unsigned long long w = 0;
         if(d.valid)
-            v = find_chain<set_, false>(T, d.key, d.h, d.c);
+            v = find_chain<set_, false>(T, d.key, d.h, d.c, w);
         if(!d.in)
             return;
         const uint64_t o = obase + d.pos;
         found[o] = d.valid ? (v ? 1 : 0) : 2;
         if constexpr(!set_)
             if(values)
-                values[o] = v ? read_val<V>(v) : V(0);
+                values[o] = v ? value_of<V>(w) : V(0);
         if(fwd)
             fwd[o] = d.valid && d.fwd;
     }
@@ -330,15 +346,15 @@ struct Seq_Reduce_Visitor
     {
         if(!d.valid)
             return;
-        const unsigned long long* v = find_chain<set_, false>(T, d.key, d.h, d.c);
-        if(!v)
+        unsigned long long w = 0;
+        if(!find_chain<set_, false>(T, d.key, d.h, d.c, w))
             return;
         if constexpr(mode_ == 0)
             acc += 1;
         else if constexpr(mode_ == 1)
-            acc += (read_val<V>(v) & (d.fwd ? m_fwd : m_rev)) != 0;
+            acc += (value_of<V>(w) & (d.fwd ? m_fwd : m_rev)) != 0;
         else
-            acc += static_cast<unsigned long long>(read_val<V>(v));
+            acc += static_cast<unsigned long long>(value_of<V>(w));
     }
     __device__ __forceinline__ void end_segment(const uint64_t q, const uint32_t lane)
     {

@@ -251,26 +251,24 @@ __device__ __forceinline__ uint32_t bucket_upsert(const Dev_Table& T, const uint
 {
     const uint8_t* csb = T.cs + b * B;
     const uint4 c0 = ld_cg4(csb), c1 = ld_cg4(csb + 16);
-    uint32_t cand = match32(c0, c1, c);
-    const uint32_t empty = match32(c0, c1, 0);
+    uint32_t cand = candidates32<true>(c0, c1, c);
     while(cand)
     {
-        const uint32_t j = __ffs(cand) - 1;
+        const uint32_t j = candidate_slot(__ffs(cand) - 1);
         cand &= cand - 1;
         if(ld_cg(key_word<set_>(T, b, j)) == key_st)
             return j_out = j, FOUND;
     }
+    const uint32_t empty = match32(c0, c1, 0);
 
+    // The claim scan: a compare-and-swap straight away (a slot with an empty checksum is most likely unclaimed), whose
+    // result, if it fails, is the racing claimer's key.
     for(uint32_t j = empty ? __ffs(empty) - 1 : B; j < B; ++j)
     {
         unsigned long long* kw = key_word<set_>(T, b, j);
-        unsigned long long cur = ld_cg(kw);
+        const unsigned long long cur = atomicCAS(kw, 0ull, key_st);
         if(cur == 0)
-        {
-            cur = atomicCAS(kw, 0ull, key_st);
-            if(cur == 0)
-                return j_out = j, INSERTED;
-        }
+            return j_out = j, INSERTED;
         if(cur == key_st)
             return j_out = j, (ld_volatile_u8(csb + j) != 0 ? FOUND : FOUND_PENDING);
     }
@@ -376,23 +374,36 @@ __device__ __forceinline__ bool await_published(const Landing& L)
 
 // Finds a key: primary bucket; absent if it is not full, or if its spill filter does not mark the minimizer; else the
 // secondary buckets; then the overflow table iff both are full (include/Streaming_Kmer_Hash_Table.hpp:2548-2574).
-// Returns the value word (the key word for a set), or null if absent.
+// Returns the value word (the key word for a set), or null if absent; a map's value word, read together with its key
+// in one 16-byte load, also goes to `val`.
 template <bool set_, bool cg_>
-__device__ __forceinline__ unsigned long long* find_chain(const Dev_Table& T, const uint64_t key, const uint64_t h, const uint8_t c)
+__device__ __forceinline__ unsigned long long* find_chain(const Dev_Table& T, const uint64_t key, const uint64_t h, const uint8_t c, unsigned long long& val)
 {
     const unsigned long long key_st = ~key;
+    // Compares the key of the slot at kw (16-byte aligned for a map), keeping its value.
+    const auto same = [&](const unsigned long long* kw) -> bool
+    {
+        if constexpr(set_)
+            return (cg_ ? ld_cg(kw) : *kw) == key_st;
+        else
+        {
+            const ulonglong2 s = cg_ ? __ldcg(reinterpret_cast<const ulonglong2*>(kw)) : *reinterpret_cast<const ulonglong2*>(kw);
+            val = s.y;
+            return s.x == key_st;
+        }
+    };
     const auto probe = [&](const uint64_t b, bool& full) -> unsigned long long*
     {
         const uint8_t* csb = T.cs + b * B;
         const uint4 c0 = cg_ ? ld_cg4(csb) : *reinterpret_cast<const uint4*>(csb);
         const uint4 c1 = cg_ ? ld_cg4(csb + 16) : *reinterpret_cast<const uint4*>(csb + 16);
-        uint32_t cand = match32(c0, c1, c);
+        uint32_t cand = candidates32<false>(c0, c1, c);
         while(cand)
         {
-            const uint32_t j = __ffs(cand) - 1;
+            const uint32_t j = candidate_slot(__ffs(cand) - 1);
             cand &= cand - 1;
             unsigned long long* kw = key_word<set_>(T, b, j);
-            if((cg_ ? ld_cg(kw) : *kw) == key_st)
+            if(same(kw))
                 return set_ ? kw : kw + 1;
         }
         full = (c1.w >> 24) != 0;   // Keys fill a bucket's slots in order: full iff its last checksum is set.
@@ -424,13 +435,30 @@ __device__ __forceinline__ unsigned long long* find_chain(const Dev_Table& T, co
     for(uint32_t t = 0; t < T.ov_probe; ++t, i = (i + 1) & T.ov_mask)
     {
         unsigned long long* kw = T.ov + 4 * i;
-        const unsigned long long cur = cg_ ? ld_cg(kw) : *kw;
-        if(cur == key_st)
-            return kw + 1;
-        if(cur == 0)
+        const ulonglong2 s = cg_ ? __ldcg(reinterpret_cast<const ulonglong2*>(kw)) : *reinterpret_cast<const ulonglong2*>(kw);
+        if(s.x == key_st)
+            return val = s.y, kw + 1;
+        if(s.x == 0)
             return nullptr;
     }
     return nullptr;
+}
+
+template <bool set_, bool cg_>
+__device__ __forceinline__ unsigned long long* find_chain(const Dev_Table& T, const uint64_t key, const uint64_t h, const uint8_t c)
+{
+    unsigned long long val;
+    return find_chain<set_, cg_>(T, key, h, c, val);
+}
+
+// The value of a found key, as read with it.
+template <typename V>
+__device__ __forceinline__ V value_of(const unsigned long long w)
+{
+    if constexpr(sizeof(V) == 8)
+        return static_cast<V>(w);
+    else
+        return static_cast<V>(static_cast<uint32_t>(w));
 }
 
 }

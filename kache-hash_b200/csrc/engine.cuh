@@ -298,10 +298,12 @@ class Engine final : public kache_table
     const uint64_t cap0_;
     uint64_t cap_, resize_th_, step_, approx_sz_ = 0, size_ = 0;
     uint64_t pending_[KACHE_MAX_USERS] = {};
+    double novelty_ = 0.5;      // Keys inserted per position in the last upsert call.
 
     // Batches.
     Pinned_Buf pin_, pin_ctr_, pin_out_;
-    cudaEvent_t ev_out_[2] = {nullptr, nullptr};
+    static constexpr int out_depth = 4;     // D2H pieces in flight ahead of the copy-out.
+    cudaEvent_t ev_out_[out_depth] = {};
     Dev_Buf dbatch_, dout_, dretry_a_, dretry_b_, dscan_, dtmp_;
 
     // Profiling.
@@ -484,37 +486,60 @@ class Engine final : public kache_table
 
     // Stages a host batch: offsets, positions and segments computed here, bases gathered into pinned memory and copied
     // in pieces, each piece's H2D copy running while the next one is gathered.
-    Batch_Info stage_host(const char* const* seqs, const size_t* lens, const size_t n)
+    // Positions per segment: short segments for the lane kernel (many lanes per batch), 512 for the warp kernel (16
+    // rows per warp); eight times longer while a sequence would have more segments than a list entry indexes.
+    static uint32_t first_seg_len(const bool lanes) { return lanes ? lane_seg_positions : seg_positions; }
+
+    static uint32_t seg_len_for(const bool lanes, const uint64_t max_pos)
     {
-        uint64_t bytes = 0, nsegs = 0, pos = 0;
+        uint64_t s = first_seg_len(lanes);
+        while((max_pos + s - 1) / s > max_seg_index + 1)
+            s *= 8;
+        return static_cast<uint32_t>(s);
+    }
+
+    Batch_Info stage_host(const char* const* seqs, const size_t* lens, const size_t n, const bool lanes)
+    {
+        uint64_t bytes = 0, max_pos = 0;
+        bool contiguous = true;
         for(size_t i = 0; i < n; ++i)
         {
             bytes += lens[i];
+            max_pos = std::max<uint64_t>(max_pos, lens[i] >= size_t(k) ? lens[i] - k + 1 : 0);
+            if(i + 1 < n && seqs[i] + lens[i] != seqs[i + 1])
+                contiguous = false;
+        }
+        // Sequences laid end to end in page-locked memory are copied to the device as they lie, with no gather.
+        const bool direct = n > 0 && bytes > 0 && contiguous && pinned(seqs[0]) && pinned(seqs[0] + bytes - 1);
+        const uint32_t seg_len = seg_len_for(lanes, max_pos);
+        uint64_t nsegs = 0;
+        for(size_t i = 0; i < n; ++i)
+        {
             const uint64_t p = lens[i] >= size_t(k) ? lens[i] - k + 1 : 0;
-            nsegs += (p + seg_positions - 1) / seg_positions, pos += p;
+            nsegs += (p + seg_len - 1) / seg_len;
         }
         const size_t o_off = 0, o_pos = o_off + (n + 1) * 8, o_seg = o_pos + (n + 1) * 8, o_bases = o_seg + nsegs * 8;
         const size_t total = o_bases + bytes + 64;
-        pin_.ensure(total);
+        pin_.ensure(direct ? o_bases + 64 : total);
         auto* off = pin_.as<uint64_t>(o_off);
         auto* pos_off = pin_.as<uint64_t>(o_pos);
         auto* segs = pin_.as<uint64_t>(o_seg);
         char* bases = pin_.as<char>(o_bases);
         // Segments listed longest first (a counting sort by length), so that the 32 lanes of a warp, which step as
         // long as their longest segment, get segments of similar lengths.
-        seg_hist_.assign(seg_positions + 1, 0);
+        seg_hist_.assign(seg_len + 1, 0);
         uint64_t b = 0, p = 0;
         for(size_t i = 0; i < n; ++i)
         {
             off[i] = b, pos_off[i] = p;
             const uint64_t np = lens[i] >= size_t(k) ? lens[i] - k + 1 : 0;
             if(np)
-                seg_hist_[seg_positions] += np / seg_positions, seg_hist_[np % seg_positions]++;
+                seg_hist_[seg_len] += np / seg_len, seg_hist_[np % seg_len]++;
             b += lens[i], p += np;
         }
         off[n] = b, pos_off[n] = p;
         seg_hist_[0] = 0;
-        for(uint64_t len = seg_positions, at = 0; len > 0; --len)
+        for(uint64_t len = seg_len, at = 0; len > 0; --len)
         {
             const uint64_t c = seg_hist_[len];
             seg_hist_[len] = at, at += c;
@@ -522,17 +547,19 @@ class Engine final : public kache_table
         for(size_t i = 0; i < n; ++i)
         {
             const uint64_t np = lens[i] >= size_t(k) ? lens[i] - k + 1 : 0;
-            for(uint64_t s = 0; s * seg_positions < np; ++s)
+            for(uint64_t s = 0; s * seg_len < np; ++s)
             {
-                const uint64_t len = std::min<uint64_t>(np - s * seg_positions, seg_positions);
+                const uint64_t len = std::min<uint64_t>(np - s * seg_len, seg_len);
                 segs[seg_hist_[len]++] = (uint64_t(i) << 24) | s;
             }
         }
         dbatch_.ensure(total);
         char* d = dbatch_.as<char>();
         check(cudaMemcpyAsync(d, pin_.p, o_bases, cudaMemcpyHostToDevice, stream_), "H2D batch");
+        if(direct)
+            check(cudaMemcpyAsync(d + o_bases, seqs[0], bytes, cudaMemcpyHostToDevice, stream_), "H2D batch");
         constexpr uint64_t piece = uint64_t(32) << 20;
-        for(size_t i0 = 0; i0 < n; )
+        for(size_t i0 = direct ? n : 0; i0 < n; )
         {
             size_t i1 = i0;
             while(i1 < n && off[i1] - off[i0] < piece)
@@ -548,13 +575,13 @@ class Engine final : public kache_table
         }
         Batch_Info bi;
         bi.b = Dev_Batch{reinterpret_cast<const uint8_t*>(d + o_bases), reinterpret_cast<const uint64_t*>(d + o_off),
-                         reinterpret_cast<const uint64_t*>(d + o_seg), reinterpret_cast<const uint64_t*>(d + o_pos), n, nsegs};
+                         reinterpret_cast<const uint64_t*>(d + o_seg), reinterpret_cast<const uint64_t*>(d + o_pos), n, nsegs, seg_len};
         bi.total_pos = p;
         return bi;
     }
 
     // Prepares a batch already in device memory: positions and segments computed on the device.
-    Batch_Info stage_dev(const uint8_t* bases, const uint64_t* off, const uint64_t n)
+    Batch_Info stage_dev(const uint8_t* bases, const uint64_t* off, const uint64_t n, const bool lanes)
     {
         const size_t o_npos = 0, o_nseg = o_npos + (n + 1) * 8, o_pos = o_nseg + (n + 1) * 8, o_sego = o_pos + (n + 1) * 8;
         const size_t head = o_sego + (n + 1) * 8;
@@ -564,28 +591,38 @@ class Engine final : public kache_table
         auto* nseg = reinterpret_cast<uint64_t*>(d + o_nseg);
         auto* pos_off = reinterpret_cast<uint64_t*>(d + o_pos);
         auto* seg_off = reinterpret_cast<uint64_t*>(d + o_sego);
-        if(n > 0)
-            launch(K_OTHER, [&](){ batch_counts_kernel<<<(n + 255) / 256, 256, 0, stream_>>>(off, n, k, npos, nseg); });
-        check(cudaMemsetAsync(pos_off, 0, 8, stream_), "memset");
-        check(cudaMemsetAsync(seg_off, 0, 8, stream_), "memset");
-        size_t tmp = 0;
-        if(n > 0)
-        {
-            check(cub::DeviceScan::InclusiveSum(nullptr, tmp, npos, pos_off + 1, static_cast<int64_t>(n), stream_), "scan");
-            dscan_.ensure(tmp);
-            check(cub::DeviceScan::InclusiveSum(dscan_.p, tmp, npos, pos_off + 1, static_cast<int64_t>(n), stream_), "scan");
-            check(cub::DeviceScan::InclusiveSum(dscan_.p, tmp, nseg, seg_off + 1, static_cast<int64_t>(n), stream_), "scan");
-        }
+        unsigned int* too_long = reinterpret_cast<unsigned int*>(ctr() + 3);
         uint64_t* h = pin_ctr_.as<uint64_t>(32);
-        check(cudaMemcpyAsync(h, pos_off + n, 8, cudaMemcpyDeviceToHost, stream_), "D2H");
-        check(cudaMemcpyAsync(h + 1, seg_off + n, 8, cudaMemcpyDeviceToHost, stream_), "D2H");
-        sync();
+        uint32_t seg_len = first_seg_len(lanes);
+        for(;;)
+        {
+            check(cudaMemsetAsync(too_long, 0, 4, stream_), "memset");
+            if(n > 0)
+                launch(K_OTHER, [&](){ batch_counts_kernel<<<(n + 255) / 256, 256, 0, stream_>>>(off, n, k, seg_len, npos, nseg, too_long); });
+            check(cudaMemsetAsync(pos_off, 0, 8, stream_), "memset");
+            check(cudaMemsetAsync(seg_off, 0, 8, stream_), "memset");
+            size_t tmp = 0;
+            if(n > 0)
+            {
+                check(cub::DeviceScan::InclusiveSum(nullptr, tmp, npos, pos_off + 1, static_cast<int64_t>(n), stream_), "scan");
+                dscan_.ensure(tmp);
+                check(cub::DeviceScan::InclusiveSum(dscan_.p, tmp, npos, pos_off + 1, static_cast<int64_t>(n), stream_), "scan");
+                check(cub::DeviceScan::InclusiveSum(dscan_.p, tmp, nseg, seg_off + 1, static_cast<int64_t>(n), stream_), "scan");
+            }
+            check(cudaMemcpyAsync(h, pos_off + n, 8, cudaMemcpyDeviceToHost, stream_), "D2H");
+            check(cudaMemcpyAsync(h + 1, seg_off + n, 8, cudaMemcpyDeviceToHost, stream_), "D2H");
+            check(cudaMemcpyAsync(h + 2, too_long, 4, cudaMemcpyDeviceToHost, stream_), "D2H");
+            sync();
+            if(!static_cast<uint32_t>(h[2]))
+                break;
+            seg_len *= 8;   // A sequence has more segments than a list entry indexes.
+        }
         const uint64_t total_pos = h[0], nsegs = h[1];
         dbatch_.ensure(nsegs * 8 + 8);
         if(n > 0)
             launch(K_OTHER, [&](){ batch_segs_kernel<<<(n + 255) / 256, 256, 0, stream_>>>(seg_off, n, dbatch_.as<uint64_t>()); });
         Batch_Info bi;
-        bi.b = Dev_Batch{bases, off, dbatch_.as<uint64_t>(), pos_off, n, nsegs};
+        bi.b = Dev_Batch{bases, off, dbatch_.as<uint64_t>(), pos_off, n, nsegs, seg_len};
         bi.total_pos = total_pos;
         return bi;
     }
@@ -609,15 +646,22 @@ class Engine final : public kache_table
 
     // The reference's per-user flush accounting over one call (include/Streaming_Kmer_Hash_Table.hpp:2248-2286,
     // 2511): fed the call's inserted keys chunk by chunk, it doubles the capacity where the reference would.
+    // The schedule's state (approximate size, capacity in buckets, resize threshold, flush step), either the
+    // engine's own or a copy for a prediction.
+    struct Sched
+    {
+        uint64_t &approx, &cap, &th, &step;
+        double lf;
+    };
+
     struct Call_Acct
     {
-        Engine& E;
-        uint32_t user;
+        Sched S;
         uint64_t pending, flushed = 0, due, ins_c = 0;
 
-        Call_Acct(Engine& E, const uint32_t u): E(E), user(u), pending(E.pending_[u])
+        Call_Acct(const Sched& S, const uint64_t pending): S(S), pending(pending)
         {
-            due = pending < E.step_ ? E.step_ - pending : 1;
+            due = pending < S.step ? S.step - pending : 1;
         }
 
         void add(const uint64_t n)
@@ -626,32 +670,77 @@ class Engine final : public kache_table
             while(due <= end)
             {
                 const uint64_t at = due;
-                E.approx_sz_ += pending + (at - flushed);
-                pending = 0, flushed = at, due = at + E.step_;
-                if(E.approx_sz_ >= E.resize_th_)
+                S.approx += pending + (at - flushed);
+                pending = 0, flushed = at, due = at + S.step;
+                if(S.approx >= S.th)
                 {
-                    if(2 * E.cap_ > max_buckets)
+                    if(2 * S.cap > max_buckets)
                         throw std::runtime_error("growing the table exceeds the most buckets supported");
-                    E.cap_ *= 2;
-                    E.resize_th_ = static_cast<uint64_t>(static_cast<double>(E.cap_ * B) * E.lf_);
-                    E.step_ = step_for(E.resize_th_);
+                    S.cap *= 2;
+                    S.th = static_cast<uint64_t>(static_cast<double>(S.cap * B) * S.lf);
+                    S.step = step_for(S.th);
                 }
             }
             ins_c = end;
         }
 
-        void finish() { E.pending_[user] = pending + (ins_c - flushed); }
+        // The user's keys inserted since its last flush, after the call.
+        uint64_t left() const { return pending + (ins_c - flushed); }
     };
+
+    // The capacity in buckets the schedule would reach if `user` inserted n more keys in one call.
+    uint64_t predicted_cap(const uint32_t user, const uint64_t n) const
+    {
+        uint64_t a = approx_sz_, c = cap_, t = resize_th_, s = step_;
+        Call_Acct sim(Sched{a, c, t, s, lf_}, pending_[user]);
+        try
+        {
+            sim.add(n);
+        }
+        catch(const std::runtime_error&)
+        {
+        }
+        return c;
+    }
+
+    // Grows the device table to `target` buckets ahead of a call's inserts: where keys sit is not observable, so the
+    // device table may have more buckets than the capacity the schedule reports, never fewer. An empty table is
+    // reallocated and zeroed rather than rebuilt. Skipped if the arrays would not fit in free device memory.
+    void grow_ahead(const uint64_t target)
+    {
+        if(target <= T_.cap)
+            return;
+        const uint64_t ov_slots = ov_slots_for(std::max<uint64_t>(1024, target));
+        const size_t need = target * (B + 32 + B * slot_bytes) + ov_slots * 32;
+        size_t free_b = 0, total_b = 0;
+        check(cudaMemGetInfo(&free_b, &total_b), "cudaMemGetInfo");
+        const size_t held = size_ == 0 ? cs_.bytes + spill_.bytes + slots_.bytes + ov_.bytes : 0;
+        if(need + (size_t(1) << 30) > free_b + held)
+            return;
+        if(size_ != 0)
+        {
+            resize(target);
+            return;
+        }
+        alloc_table(cs_, spill_, slots_, target);
+        bind(T_, cs_, spill_, slots_, target);
+        ov_slots_ = ov_slots;
+        set_ov(T_, ov_, ov_slots_);
+        check(cudaMemsetAsync(ctr() + 1, 0, sizeof(unsigned long long), stream_), "memset");
+    }
 
     // Upserts a staged batch with the value functor `fn`, chunk by chunk (see the top of this file).
     template <typename Fn> uint64_t run_upsert(const uint32_t user, const Batch_Info& bi, const Fn& fn)
     {
-        Call_Acct acct(*this, user);
         const uint64_t nsegs = bi.b.nsegs;
         const double pos_per_seg = nsegs ? static_cast<double>(bi.total_pos) / nsegs : 1.0;
         uint64_t total_ins = 0;
-        // Keys inserted per position: assumed 1/2 for the first chunk, then as the last chunk measured.
-        double novelty = 0.5;
+        // Keys inserted per position: as the previous call measured (1/2 before the first), then as the last chunk
+        // measured. The device table is first grown to the capacity the schedule would reach at that rate, so that
+        // a call usually runs as one launch, with no rebuild.
+        double novelty = novelty_;
+        grow_ahead(predicted_cap(user, static_cast<uint64_t>(novelty * static_cast<double>(bi.total_pos))));
+        Call_Acct acct(Sched{approx_sz_, cap_, resize_th_, step_, lf_}, pending_[user]);
         const size_t bits = bi.total_pos / 8 + 8;
         unsigned int* retried = reinterpret_cast<unsigned int*>(ctr() + 2);
 
@@ -663,10 +752,11 @@ class Engine final : public kache_table
                 check(cudaMemsetAsync(dretry_a_.p, 0, dretry_a_.bytes, stream_), "memset");
                 dretry_dirty_ = false;
             }
-            // A chunk may take the table to 95 % of its slots; the schedule then resizes it, as the reference would.
-            const double slots = static_cast<double>(cap_ * B);
+            // A chunk may take the device table to 95 % of its slots, at a quarter above the expected rate; the
+            // schedule then resizes it, as the reference would.
+            const double slots = static_cast<double>(T_.cap * B);
             const double room = std::max(0.95 * slots - static_cast<double>(size_), 0.05 * slots);
-            const double want_pos = room / std::max(novelty, 1e-3);
+            const double want_pos = room / std::max(1.25 * novelty, 1e-3);
             uint64_t se = sb + std::max<uint64_t>(1, static_cast<uint64_t>(want_pos / pos_per_seg));
             if(se + (se - sb) / 2 >= nsegs)
                 se = nsegs;     // No small last chunk: it would run with too few lanes to fill the GPU.
@@ -695,14 +785,15 @@ class Engine final : public kache_table
             novelty = chunk_pos > 0 ? std::max(static_cast<double>(ins) / chunk_pos, 1e-3) : novelty;
             size_ += ins, total_ins += ins;
             acct.add(ins);
-            const uint64_t gpu_cap = T_.cap;
-            if(cap_ != gpu_cap)
+            if(cap_ > T_.cap)
                 resize(cap_);
             if(c[1] * 4 > ov_slots_ * 3)
                 grow_overflow();
             sb = se;
         }
-        acct.finish();
+        pending_[user] = acct.left();
+        if(bi.total_pos > 0)
+            novelty_ = std::max(static_cast<double>(total_ins) / static_cast<double>(bi.total_pos), 1e-3);
         return total_ins;
     }
 
@@ -731,34 +822,56 @@ class Engine final : public kache_table
             stream_launch(K_REDUCE, bi, 0, bi.b.nsegs, Seq_Reduce_Visitor<set_, VT, 2>{T_, out, VT(mf), VT(mr), 0, 0});
     }
 
-    // Copies device output to a host buffer through pinned memory, in pieces, the copy-out overlapping the next D2H.
-    // Copies device output to a host buffer through two pinned pieces: piece i's D2H copy runs while piece i - 1
-    // is copied out to the caller's buffer by the host pool.
+    // Whether host memory at p is page-locked (the caller's cudaHostAlloc'd or registered memory): copies then use it
+    // directly.
+    static bool pinned(const void* p)
+    {
+        if(p == nullptr)
+            return false;
+        cudaPointerAttributes a{};
+        if(cudaPointerGetAttributes(&a, p) != cudaSuccess)
+        {
+            (void)cudaGetLastError();
+            return false;
+        }
+        return a.type == cudaMemoryTypeHost;
+    }
+
+    // Copies device output to a host buffer. Into page-locked memory, one copy. Into pageable memory, through pinned
+    // pieces: up to `out_depth` D2H copies run ahead while the host pool copies finished pieces out.
     void d2h(void* dst, const void* src, const size_t bytes)
     {
         if(bytes == 0)
             return;
+        if(pinned(dst) && pinned(static_cast<char*>(dst) + bytes - 1))
+        {
+            check(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, stream_), "D2H");
+            sync();
+            return;
+        }
         constexpr size_t piece = size_t(32) << 20;
-        pin_out_.ensure(2 * piece);
+        pin_out_.ensure(out_depth * piece);
         if(!ev_out_[0])
-            check(cudaEventCreateWithFlags(&ev_out_[0], cudaEventDisableTiming), "event"), check(cudaEventCreateWithFlags(&ev_out_[1], cudaEventDisableTiming), "event");
-        char* stage[2] = {pin_out_.as<char>(0), pin_out_.as<char>(piece)};
+            for(auto& e : ev_out_)
+                check(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "event");
         const size_t pieces = (bytes + piece - 1) / piece;
-        const auto copy_out = [&](const size_t i)
+        const auto issue = [&](const size_t i)
         {
             const size_t o = i * piece, m = std::min(piece, bytes - o);
-            check(cudaEventSynchronize(ev_out_[i & 1]), "event sync");
-            parallel_for(m, size_t(2) << 20, [&](const size_t s, const size_t e){ std::memcpy(static_cast<char*>(dst) + o + s, stage[i & 1] + s, e - s); });
+            check(cudaMemcpyAsync(pin_out_.as<char>((i % out_depth) * piece), static_cast<const char*>(src) + o, m, cudaMemcpyDeviceToHost, stream_), "D2H");
+            check(cudaEventRecord(ev_out_[i % out_depth], stream_), "event record");
         };
+        for(size_t i = 0; i < std::min<size_t>(out_depth, pieces); ++i)
+            issue(i);
         for(size_t i = 0; i < pieces; ++i)
         {
             const size_t o = i * piece, m = std::min(piece, bytes - o);
-            check(cudaMemcpyAsync(stage[i & 1], static_cast<const char*>(src) + o, m, cudaMemcpyDeviceToHost, stream_), "D2H");
-            check(cudaEventRecord(ev_out_[i & 1], stream_), "event record");
-            if(i > 0)
-                copy_out(i - 1);
+            const char* stage = pin_out_.as<char>((i % out_depth) * piece);
+            check(cudaEventSynchronize(ev_out_[i % out_depth]), "event sync");
+            parallel_for(m, size_t(1) << 20, [&](const size_t s, const size_t e){ std::memcpy(static_cast<char*>(dst) + o + s, stage + s, e - s); });
+            if(i + out_depth < pieces)
+                issue(i + out_depth);
         }
-        copy_out(pieces - 1);
     }
 
     static Op_Fn<VT> op_fn(const uint32_t op, const uint64_t x, const uint64_t init) { return Op_Fn<VT>{op, static_cast<VT>(x), static_cast<VT>(init)}; }
@@ -814,7 +927,7 @@ public:
     uint64_t upsert(uint32_t user, const char* const* seqs, const size_t* lens, size_t n, uint32_t op, uint64_t x, uint64_t init) override
     {
         std::lock_guard<std::mutex> g(work);
-        const auto bi = stage_host(seqs, lens, n);
+        const auto bi = stage_host(seqs, lens, n, true);
         return run_upsert(user, bi, op_fn(op, x, init));
     }
 
@@ -825,7 +938,7 @@ public:
         else
         {
             std::lock_guard<std::mutex> g(work);
-            const auto bi = stage_host(seqs, lens, n);
+            const auto bi = stage_host(seqs, lens, n, true);
             return run_upsert(user, bi, Oriented_Op_Fn<VT>{op, static_cast<VT>(xf), static_cast<VT>(xr)});
         }
     }
@@ -837,7 +950,7 @@ public:
         else
         {
             std::lock_guard<std::mutex> g(work);
-            const auto bi = stage_host(seqs, lens, n);
+            const auto bi = stage_host(seqs, lens, n, true);
             return run_update(bi, op_fn(op, x, 0));
         }
     }
@@ -845,7 +958,7 @@ public:
     void lookup(const char* const* seqs, const size_t* lens, size_t n, uint8_t* found, void* values, uint8_t* fwd) override
     {
         std::lock_guard<std::mutex> g(work);
-        const auto bi = stage_host(seqs, lens, n);
+        const auto bi = stage_host(seqs, lens, n, false);
         const uint64_t P = bi.total_pos;
         const size_t vb = (!set_ && values) ? sizeof(VT) : 0;
         const size_t a_found = (P + 15) / 16 * 16, a_val = (P * vb + 15) / 16 * 16;
@@ -864,7 +977,7 @@ public:
     void seq_reduce(const char* const* seqs, const size_t* lens, size_t n, int mode, uint64_t m_fwd, uint64_t m_rev, uint64_t* out) override
     {
         std::lock_guard<std::mutex> g(work);
-        const auto bi = stage_host(seqs, lens, n);
+        const auto bi = stage_host(seqs, lens, n, true);
         dout_.ensure(n * 8 + 8);
         run_seq_reduce(bi, mode, m_fwd, m_rev, dout_.as<unsigned long long>());
         d2h(out, dout_.p, n * 8);
@@ -873,7 +986,7 @@ public:
     void describe(const char* const* seqs, const size_t* lens, size_t n, uint64_t* key, uint64_t* h, uint8_t* cs, uint8_t* fwd, uint8_t* valid) override
     {
         std::lock_guard<std::mutex> g(work);
-        const auto bi = stage_host(seqs, lens, n);
+        const auto bi = stage_host(seqs, lens, n, false);
         const uint64_t P = bi.total_pos;
         dout_.ensure(P * 19 + 64);
         auto* dk = dout_.as<uint64_t>();
@@ -886,7 +999,7 @@ public:
     uint64_t upsert_dev(uint32_t user, const uint8_t* b, const uint64_t* off, uint64_t n, uint32_t op, uint64_t x, uint64_t init) override
     {
         std::lock_guard<std::mutex> g(work);
-        const auto bi = stage_dev(b, off, n);
+        const auto bi = stage_dev(b, off, n, true);
         return run_upsert(user, bi, op_fn(op, x, init));
     }
 
@@ -897,7 +1010,7 @@ public:
         else
         {
             std::lock_guard<std::mutex> g(work);
-            const auto bi = stage_dev(b, off, n);
+            const auto bi = stage_dev(b, off, n, true);
             return run_upsert(user, bi, Oriented_Op_Fn<VT>{op, static_cast<VT>(xf), static_cast<VT>(xr)});
         }
     }
@@ -909,7 +1022,7 @@ public:
         else
         {
             std::lock_guard<std::mutex> g(work);
-            const auto bi = stage_dev(b, off, n);
+            const auto bi = stage_dev(b, off, n, true);
             return run_update(bi, op_fn(op, x, 0));
         }
     }
@@ -917,7 +1030,7 @@ public:
     void lookup_dev(const uint8_t* b, const uint64_t* off, uint64_t n, uint8_t* found, void* values, uint8_t* fwd) override
     {
         std::lock_guard<std::mutex> g(work);
-        const auto bi = stage_dev(b, off, n);
+        const auto bi = stage_dev(b, off, n, false);
         run_lookup(bi, found, set_ ? nullptr : static_cast<VT*>(values), fwd);
         sync();
     }
@@ -925,7 +1038,7 @@ public:
     void count_dev(const uint8_t* b, const uint64_t* off, uint64_t n, uint64_t* counts) override
     {
         std::lock_guard<std::mutex> g(work);
-        const auto bi = stage_dev(b, off, n);
+        const auto bi = stage_dev(b, off, n, true);
         run_seq_reduce(bi, 0, 0, 0, reinterpret_cast<unsigned long long*>(counts));
         sync();
     }
@@ -964,7 +1077,7 @@ public:
         std::lock_guard<std::mutex> g(work);
         unsigned long long* out = ctr() + 3;
         check(cudaMemsetAsync(out, 0, 8, stream_), "memset");
-        const uint64_t total = cap_ * B + ov_slots_;
+        const uint64_t total = T_.cap * B + ov_slots_;
         launch(K_OTHER, [&](){ reduce_kernel<set_, VT><<<grid_for(total / 32 + 1, 8), 256, 0, stream_>>>(T_, what, mask, out, 0, nullptr); });
         return read_ctr(4)[3];
     }
@@ -974,7 +1087,7 @@ public:
         std::lock_guard<std::mutex> g(work);
         dout_.ensure((max + 1) * 8);
         check(cudaMemsetAsync(dout_.p, 0, (max + 1) * 8, stream_), "memset");
-        const uint64_t total = cap_ * B + ov_slots_;
+        const uint64_t total = T_.cap * B + ov_slots_;
         launch(K_OTHER, [&](){ reduce_kernel<set_, VT><<<grid_for(total / 32 + 1, 8), 256, 0, stream_>>>(T_, 3, 0, ctr() + 3, max, dout_.as<unsigned long long>()); });
         d2h(h, dout_.p, (max + 1) * 8);
         h[0] = 0;
@@ -983,7 +1096,7 @@ public:
     void for_each(uint32_t shards, uint32_t shard, kache_keys_fn f, void* ctx) override
     {
         std::lock_guard<std::mutex> g(work);
-        const uint64_t bb = cap_ * shard / shards, be = cap_ * (shard + 1) / shards;
+        const uint64_t bb = T_.cap * shard / shards, be = T_.cap * (shard + 1) / shards;
         const uint64_t ov_range = (ov_slots_ + shards - 1) / shards;
         const uint64_t ob = std::min<uint64_t>(ov_range * shard, ov_slots_), oe = std::min<uint64_t>(ov_range * (shard + 1), ov_slots_);
         constexpr uint64_t piece = uint64_t(1) << 18;   // Buckets per device pass.
@@ -1027,11 +1140,11 @@ public:
         std::lock_guard<std::mutex> g(work);
         out = kache_stats{};
         out.capacity = cap_ * B;
-        out.bytes = cap_ * (B + 32 + B * slot_bytes);
+        out.bytes = T_.cap * (B + 32 + B * slot_bytes) + ov_slots_ * 32;
         out.keys = size_;
         unsigned long long* ps = ctr() + 3;
         check(cudaMemsetAsync(ps, 0, 16, stream_), "memset");
-        launch(K_OTHER, [&](){ distribution_kernel<k, l, set_><<<grid_for(cap_ * B / 32 + 1, 8), 256, 0, stream_>>>(T_, ps); });
+        launch(K_OTHER, [&](){ distribution_kernel<k, l, set_><<<grid_for(T_.cap * B / 32 + 1, 8), 256, 0, stream_>>>(T_, ps); });
         const auto* c = read_ctr(5);
         out.overflow_keys = c[1];
         const double p = static_cast<double>(c[3]), s = static_cast<double>(c[4]), o = static_cast<double>(c[1]);
@@ -1047,14 +1160,14 @@ public:
     template <typename Fn> uint64_t upsert_with(const uint32_t user, const char* const* seqs, const size_t* lens, const size_t n, const Fn& fn)
     {
         std::lock_guard<std::mutex> g(work);
-        const auto bi = stage_host(seqs, lens, n);
+        const auto bi = stage_host(seqs, lens, n, true);
         return run_upsert(user, bi, fn);
     }
 
     template <typename Fn> uint64_t update_with(const char* const* seqs, const size_t* lens, const size_t n, const Fn& fn)
     {
         std::lock_guard<std::mutex> g(work);
-        const auto bi = stage_host(seqs, lens, n);
+        const auto bi = stage_host(seqs, lens, n, true);
         return run_update(bi, fn);
     }
 

@@ -357,4 +357,24 @@ double ref_bench_count(void* tv, const char* bases, const uint64_t* off, uint64_
     return now_s() - t0;
 }
 
+
+// Per-position finds (found flag and value at pos_off[q] + i), in batches of `batch` sequences over `threads`
+// threads; returns the wall seconds.
+double ref_bench_lookup(void* tv, const char* bases, const uint64_t* off, uint64_t n, const uint64_t* pos_off, uint32_t batch, uint32_t threads, uint8_t* found, uint64_t* val)
+{
+    auto* t = static_cast<Table*>(tv);
+    std::atomic<uint64_t> next{0};
+    const double t0 = now_s();
+    std::vector<std::thread> W;
+    for(uint32_t w = 0; w < threads; ++w)
+        W.emplace_back([&]()
+        {
+            for(uint64_t b; (b = next++) * batch < n; )
+                t->lookup(Batch(bases, off, n, b * batch, (b + 1) * batch), pos_off + b * batch, found, val, nullptr);
+        });
+    for(auto& w : W)
+        w.join();
+    return now_s() - t0;
+}
+
 }

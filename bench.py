@@ -16,6 +16,7 @@ workload with all host threads.
 import argparse
 import json
 import os
+import re
 import sys
 import threading
 import time
@@ -123,6 +124,33 @@ def max_over_ranks(dist, x, device):
     t = torch.tensor([x], dtype=torch.float64, device=device)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
+
+
+def ncu_traffic(kernel):
+    """DRAM bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum) of the kernel on this workload, from the
+    committed ncu summary under profiles/, or None."""
+    name = {"lookup": "lookup_stream_kernel_config1.md", "upsert": "upsert_lane_kernel_config1.md"}.get(kernel)
+    try:
+        with open(os.path.join(os.path.dirname(os.path.abspath(__file__)), "profiles", name)) as f:
+            m = re.search(r"\| dram bytes per launch \| (\d+) \|", f.read())
+        return int(m.group(1)) if m else None
+    except (OSError, TypeError):
+        return None
+
+
+def random_roofs(kache, nbytes=4 << 30):
+    """The device's random-access roofs (kache_b200_memory_roof): 32-byte sector reads and atomic updates at random
+    over `nbytes`, and the dependent-load latency."""
+    try:
+        _, rd = kache.memory_roof(nbytes, kache.ROOF_RANDOM_READ, 1 << 28)
+        _, up = kache.memory_roof(nbytes, kache.ROOF_RANDOM_UPDATE, 1 << 28)
+        _, seq = kache.memory_roof(nbytes, kache.ROOF_SEQ_READ, 0)
+        threads, per = 148 * 8 * 256, 64
+        ms, ch = kache.memory_roof(nbytes, kache.ROOF_CHASE, threads * per)
+        return {"array_bytes": nbytes, "read_sectors_per_s": rd, "read_gbs": rd * 32 / 1e9, "update_per_s": up,
+                "update_gbs_rmw": up * 64 / 1e9, "seq_read_gbs": seq / 1e9, "chase_latency_ns": 1e6 * ms / per}
+    except Exception as e:  # noqa: BLE001
+        return {"error": str(e)}
 
 
 def positions(off, k=31):
@@ -314,6 +342,17 @@ def run_b200(args):
     }
     for kv in kernels.values():
         kv["achieved_gbs"] = kv["bytes_per_launch"] / (kv["ms_total"] / max(1, kv["launches"]) * 1e-3) / 1e9 if kv["ms_total"] else None
+    # The random-access roofline: a launch's streamed bytes at the copy peak plus its random sector reads and updates
+    # at the device's measured random-sector rates (kache_b200_memory_roof over a 4 GiB array).
+    roof = random_roofs(kache) if rank == 0 else None
+    if roof and "error" not in roof:
+        streamed = {"upsert": b_in_up * P_up, "lookup": (b_in_find + 9) * P_find}
+        reads = {"upsert": P_up * (rho + (1 - inserted / P_up)), "lookup": P_find * (rho + hit)}
+        updates = {"upsert": P_up * 1.0, "lookup": 0.0}
+        for name_, kv in kernels.items():
+            t_roof = streamed[name_] / (peak * 1e9) + reads[name_] / roof["read_sectors_per_s"] + updates[name_] / roof["update_per_s"]
+            kv["random_roof_ms"] = 1e3 * t_roof
+            kv["frac_of_random_roof"] = (1e3 * t_roof) / (kv["ms_total"] / max(1, kv["launches"])) if kv["ms_total"] else None
     dom = max(kernels, key=lambda k_: kernels[k_]["ms_total"])
     d = kernels[dom]
 
@@ -354,8 +393,9 @@ def run_b200(args):
                        "l2": "inputs larger than L2 (reads 250 MB + table 240 MB per step)", "parallelism": f"{ws} independent tables"},
             "gpu_launches": launches,
             "roofline": {"bound": "hbm", "kernel": dom, "achieved": d["achieved_gbs"], "peak": peak, "unit": "GB/s",
-                         "frac": (d["achieved_gbs"] / peak) if d["achieved_gbs"] else None, "traffic": None,
-                         "peak_source": peak_kind, "kernels": kernels,
+                         "frac": (d["achieved_gbs"] / peak) if d["achieved_gbs"] else None, "traffic": ncu_traffic(dom),
+                         "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one launch on this workload (profiles/)",
+                         "peak_source": peak_kind, "kernels": kernels, "random_roof": roof,
                          "model": "A = b_in + b_out + 32*rho + 32*r_slot + 32*w_slot bytes per k-mer; rho from the describer on 5000 reads"},
             "e2e": {"value": P * ws / (e2e_ms * 1e-3), "unit": "k-mers/s", "ms_per_step": e2e_ms,
                     "h2d_bytes_per_step": int(bi.off[-1] + bh.off[-1] + 16 * (bi.n + bh.n)),

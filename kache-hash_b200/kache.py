@@ -91,6 +91,7 @@ def lib():
             "kache_b200_profile": (ctypes.c_int, [_vp, ctypes.c_int]),
             "kache_b200_profile_read": (ctypes.c_int, [_vp, ctypes.c_uint32, ctypes.POINTER(ctypes.c_double), _u64p]),
             "kache_b200_kernel_launches": (ctypes.c_uint64, []),
+            "kache_b200_memory_roof": (ctypes.c_int, [ctypes.c_uint64, ctypes.c_uint32, ctypes.c_uint64, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)]),
         }
         for name, (res, args) in sig.items():
             f = getattr(L, name)
@@ -377,3 +378,13 @@ class Counter:
 
 def kernel_launches():
     return lib().kache_b200_kernel_launches()
+
+
+ROOF_SEQ_READ, ROOF_RANDOM_READ, ROOF_RANDOM_UPDATE, ROOF_CHASE = 0, 1, 2, 3
+
+
+def memory_roof(nbytes, kind, accesses=1 << 27):
+    """(ms, rate) of one of the device's memory roofs (kache_b200_memory_roof)."""
+    ms, rate = ctypes.c_double(), ctypes.c_double()
+    _check(lib().kache_b200_memory_roof(nbytes, kind, accesses, ctypes.byref(ms), ctypes.byref(rate)), "kache_b200_memory_roof")
+    return ms.value, rate.value

@@ -138,14 +138,14 @@ def ncu_traffic(kernel):
         return None
 
 
-def random_roofs(kache, nbytes=4 << 30):
+def random_roofs(kache, nbytes=1 << 30):
     """The device's random-access roofs (kache_b200_memory_roof): 32-byte sector reads and atomic updates at random
     over `nbytes`, and the dependent-load latency."""
     try:
         _, rd = kache.memory_roof(nbytes, kache.ROOF_RANDOM_READ, 1 << 28)
         _, up = kache.memory_roof(nbytes, kache.ROOF_RANDOM_UPDATE, 1 << 28)
         _, seq = kache.memory_roof(nbytes, kache.ROOF_SEQ_READ, 0)
-        threads, per = 148 * 8 * 256, 64
+        threads, per = 148 * 32, 256
         ms, ch = kache.memory_roof(nbytes, kache.ROOF_CHASE, threads * per)
         return {"array_bytes": nbytes, "read_sectors_per_s": rd, "read_gbs": rd * 32 / 1e9, "update_per_s": up,
                 "update_gbs_rmw": up * 64 / 1e9, "seq_read_gbs": seq / 1e9, "chase_latency_ns": 1e6 * ms / per}
@@ -178,12 +178,12 @@ def cpu_baseline_sample(ins, held, threads):
             "sample": f"upsert {si.n} reads + per-position find over {sh.n} held-out reads ({p} positions), batches of 64 reads, {threads} threads"}
 
 
-def ref_lookup_timed(L, t, b, threads):
+def ref_lookup_timed(L, t, b, threads, k=31):
     """Seconds for the reference's per-position find over batch b (found flags and values into host arrays, as
     kache_lookup returns them)."""
     lens = np.diff(b.off).astype(np.int64)
     pos_off = np.zeros(b.n + 1, np.uint64)
-    np.cumsum(np.maximum(lens - 30, 0), out=pos_off[1:])
+    np.cumsum(np.maximum(lens - k + 1, 0), out=pos_off[1:])
     P = int(pos_off[-1])
     found = np.zeros(max(P, 1), np.uint8)
     vals = np.zeros(max(P, 1), np.uint64)
@@ -342,12 +342,13 @@ def run_b200(args):
     }
     for kv in kernels.values():
         kv["achieved_gbs"] = kv["bytes_per_launch"] / (kv["ms_total"] / max(1, kv["launches"]) * 1e-3) / 1e9 if kv["ms_total"] else None
-    # The random-access roofline: a launch's streamed bytes at the copy peak plus its random sector reads and updates
-    # at the device's measured random-sector rates (kache_b200_memory_roof over a 4 GiB array).
+    # The random-access roofline: a launch's streamed bytes at the copy peak plus its random slot-sector reads and
+    # updates at the device's measured random-sector rates (kache_b200_memory_roof over a 1 GiB array, larger than the
+    # table); the checksum sectors (the 32*rho term) are left out, as the checksum array (25 MB) stays in L2.
     roof = random_roofs(kache) if rank == 0 else None
     if roof and "error" not in roof:
         streamed = {"upsert": b_in_up * P_up, "lookup": (b_in_find + 9) * P_find}
-        reads = {"upsert": P_up * (rho + (1 - inserted / P_up)), "lookup": P_find * (rho + hit)}
+        reads = {"upsert": P_up * (1 - inserted / P_up), "lookup": P_find * hit}
         updates = {"upsert": P_up * 1.0, "lookup": 0.0}
         for name_, kv in kernels.items():
             t_roof = streamed[name_] / (peak * 1e9) + reads[name_] / roof["read_sectors_per_s"] + updates[name_] / roof["update_per_s"]
@@ -429,16 +430,242 @@ def run_density(kache, b):
     return float(runs.sum()) / max(1, int(valid.sum()))
 
 
+# ---- The other workloads: one JSON line each, for the record (the default line is config 1) -----------------------
+
+def dev_batch(b, dev):
+    """A batch's bases and offsets copied to the device: (tensors, n)."""
+    import torch
+    return torch.from_numpy(b.bases).to(dev), torch.from_numpy(b.off.view(np.int64)).to(dev), b.n
+
+
+def dev_pieces(b, dev, per):
+    """The batch cut into sub-batches of `per` sequences on the device, each with offsets of its own."""
+    import torch
+    out = []
+    for s in range(0, b.n, per):
+        e = min(b.n, s + per)
+        o0 = int(b.off[s])
+        off = (b.off[s:e + 1] - np.uint64(o0)).view(np.int64)
+        out.append((torch.from_numpy(b.bases[o0:int(b.off[e]) + 16].copy()).to(dev), torch.from_numpy(off.copy()).to(dev), e - s))
+    return out
+
+
+def timed_steps(stream, step, steps, warmup):
+    """Mean device milliseconds per step, CUDA events on the stream, after `warmup` untimed steps."""
+    import torch
+    for _ in range(warmup):
+        step()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(steps):
+        step()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / steps
+
+
+def pinned_copy(b):
+    import torch
+    from kache import Batch
+    t = torch.empty(b.bases.nbytes, dtype=torch.uint8, pin_memory=True)
+    t.numpy()[:] = b.bases
+    pb = Batch(t.numpy(), b.off)
+    pb.keep = t
+    return pb
+
+
+def ref_sample(kind, n, lf, pow2, calls):
+    """Seconds the reference's own table (oracle/_ref) takes for `calls`, a list of (function name, batch, args),
+    all host threads; None where it was not built."""
+    import oracle
+    L = oracle.ref()
+    if L is None:
+        return None, 0
+    threads = min(128, os.cpu_count() or 1)
+    t = L.ref_new(kind, n, lf, 1 if pow2 else 0, threads)
+    out = oracle._u64()
+    total = 0.0
+    for fn, b, a in calls:
+        if fn == "lookup":
+            total += ref_lookup_timed(L, t, b, threads, *a)
+        else:
+            total += getattr(L, fn)(t, b.bases.ctypes.data, b.off.ctypes.data, b.n, 64, threads, *a, oracle.ctypes.byref(out))
+    L.ref_free(t)
+    return total, threads
+
+
+def config_line(metric, value, ms, cfg, e2e=None, cpu=None, extra=None):
+    line = {"metric": metric, "value": value, "unit": "k-mers/s", "n_gpus": 1, "ms_per_step": ms, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "data": "synthetic", "config": cfg, "e2e": e2e, "cpu_baseline": cpu}
+    line.update(extra or {})
+    print(json.dumps(line))
+
+
+def run_config2(args):
+    """Kmer_Set_Counter, <31, u32, 22> at load factor 0.9, power-of-2 capacity: prime with the genome's 31-mers
+    (upsert KEEP, initial 0), count the reads (present-only wrapping +1), histogram(10000)."""
+    import torch
+    import kache
+    from kache import Batch
+    dev = torch.device("cuda", 0)
+    stream = torch.cuda.current_stream()
+    g, index, reads = synth.config2(args.scale)
+    bi, br = Batch(*index), Batch(*reads)
+    n = int(100_000_000 * args.scale)
+    P = positions(bi.off) + positions(br.off)
+    T = kache.Table(31, 4, n, 0.9, True)
+    T.set_stream(stream.cuda_stream)
+    u = T.register()
+    (ib, io, ni), (rb, ro, nr) = dev_batch(bi, dev), dev_batch(br, dev)
+    hist = {}
+
+    def step():
+        T.clear()
+        T.upsert_dev(u, ib.data_ptr(), io.data_ptr(), ni, kache.KEEP, 0, 0)
+        hist["found"] = T.update_dev(rb.data_ptr(), ro.data_ptr(), nr, kache.ADD_WRAP, 1)
+        hist["h"] = T.histogram(10000)
+
+    ms = timed_steps(stream, step, args.steps, args.warmup)
+    size, cap = T.size(), T.capacity()
+    T.close()
+    # End to end through the counter's C interface with page-locked host batches.
+    pi, pr = pinned_copy(bi), pinned_copy(br)
+    C = kache.Counter(n, 16, 0.9)
+    t0 = time.perf_counter()
+    C.prime_batch(pi)
+    C.count_batch(pr)
+    C.histogram(10000)
+    e2e_ms = 1000 * (time.perf_counter() - t0)
+    C.close()
+    # The reference on a twentieth of the reads (after priming with the whole genome, untimed for the sample rate).
+    rs = br.slice(0, br.n // 20)
+    t_ref, threads = ref_sample(1, n, 0.9, True, [("ref_bench_upsert", bi, (0, 0)), ("ref_bench_update", rs, (16, 1))])
+    cpu = None if t_ref is None else {"value": (positions(bi.off) + positions(rs.off)) / t_ref, "unit": "k-mers/s", "cores": threads,
+                                      "kind": "reference", "sample": f"prime with the whole index, count {rs.n} of {br.n} reads"}
+    config_line("k-mers/s prime+count (config 2: Kmer_Set_Counter <31,u32,22>, lf 0.9 pow2)", P / (ms * 1e-3), ms,
+                {"workload": f"config 2 at scale {args.scale}: {len(g)} bp genome (5% segmental duplications), {br.n} reads "
+                             "lognormal(150, 0.6) clipped 50-1000 bp at 30x", "prime_positions": positions(bi.off),
+                 "count_positions": positions(br.off), "keys": size, "capacity": cap, "found": hist["found"],
+                 "histogram_sum": int(sum(hist["h"]))},
+                e2e={"value": P / (e2e_ms * 1e-3), "unit": "k-mers/s", "ms_per_step": e2e_ms, "host_buffers": "page-locked",
+                     "calls": "kache_counter_prime_batch, kache_counter_count_batch, kache_counter_histogram"},
+                cpu=cpu)
+
+
+def run_config3(args):
+    """Oriented strand map <27, u8, 16>: upsert_oriented(OR, fwd 1, rev 2) of long reads with indels, then per-position
+    find with the orientation; all reads in one call, and in calls of 256 reads."""
+    import torch
+    import kache
+    from kache import Batch
+    dev = torch.device("cuda", 0)
+    stream = torch.cuda.current_stream()
+    g, reads = synth.config3(args.scale)
+    br = Batch(*reads)
+    n = int(50_000_000 * args.scale)
+    P1 = positions(br.off, 27)
+    T = kache.Table(27, 1, n, 0.8, False)
+    T.set_stream(stream.cuda_stream)
+    u = T.register()
+    rb, ro, nr = dev_batch(br, dev)
+    found = torch.empty(P1, dtype=torch.uint8, device=dev)
+    vals = torch.empty(P1, dtype=torch.uint8, device=dev)
+    fwd = torch.empty(P1, dtype=torch.uint8, device=dev)
+
+    def step():
+        T.clear()
+        T.upsert_oriented_dev(u, rb.data_ptr(), ro.data_ptr(), nr, kache.OR, 1, 2)
+        T.lookup_dev(rb.data_ptr(), ro.data_ptr(), nr, found.data_ptr(), vals.data_ptr(), fwd.data_ptr())
+
+    ms = timed_steps(stream, step, args.steps, args.warmup)
+    pieces = dev_pieces(br, dev, 256)
+    starts = np.concatenate([[0], np.cumsum([int(np.maximum(np.diff(o_.cpu().numpy()) - 26, 0).sum()) for _, o_, _ in pieces])])
+
+    def step_batched():
+        T.clear()
+        for b_, o_, n_ in pieces:
+            T.upsert_oriented_dev(u, b_.data_ptr(), o_.data_ptr(), n_, kache.OR, 1, 2)
+        for i_, (b_, o_, n_) in enumerate(pieces):
+            at = int(starts[i_])
+            T.lookup_dev(b_.data_ptr(), o_.data_ptr(), n_, found[at:].data_ptr(), vals[at:].data_ptr(), fwd[at:].data_ptr())
+
+    ms_b = timed_steps(stream, step_batched, max(1, args.steps // 3), 1)
+    T.profile(True)
+    step_batched()
+    torch.cuda.synchronize()
+    prof_b = {kind: T.profile_read(i) for i, kind in enumerate(["upsert", "update", "lookup", "reduce", "resize", "other"])}
+    T.profile(False)
+    size, cap = T.size(), T.capacity()
+    T.close()
+    t_ref, threads = ref_sample(5, n, 0.8, False, [("ref_bench_upsert_oriented", br, (3, 1, 2)), ("lookup", br, (27,))])
+    cpu = None if t_ref is None else {"value": 2 * P1 / t_ref, "unit": "k-mers/s", "cores": threads, "kind": "reference",
+                                      "sample": "the whole workload once"}
+    config_line("k-mers/s upsert_oriented+find (config 3: <27,u8,16> strand map, long reads)", 2 * P1 / (ms * 1e-3), ms,
+                {"workload": f"config 3 at scale {args.scale}: {len(g)} bp genome, {br.n} reads lognormal(10 kb, 0.8) clipped "
+                             "1-100 kb at 5x, 5% errors 3:1:1", "positions_per_phase": P1, "keys": size, "capacity": cap},
+                cpu=cpu, extra={"batched_256_reads": {"value": 2 * P1 / (ms_b * 1e-3), "ms_per_step": ms_b, "calls_per_step": 2 * len(pieces),
+                                                      "kernel_ms_one_step": {k_: v_[0] for k_, v_ in prof_b.items()}}})
+
+
+def run_config4(args):
+    """Resize-heavy set <32, void, 20> sized for 1M keys (load factor 0.8, exact capacity): insert a uniform genome
+    streamed as 150 bp pieces at 1x, in calls of 65,536 pieces; the table doubles about 9 times per step."""
+    import torch
+    import kache
+    from kache import Batch
+    dev = torch.device("cuda", 0)
+    stream = torch.cuda.current_stream()
+    g, pieces_ = synth.config4(args.scale)
+    bs = Batch(*pieces_)
+    P = positions(bs.off, 32)
+    T = kache.Table(32, 0, 1_000_000, 0.8, False)
+    T.set_stream(stream.cuda_stream)
+    u = T.register()
+    pieces = dev_pieces(bs, dev, 65536)
+    ins = {}
+
+    def step():
+        T.clear()
+        c = 0
+        for b_, o_, n_ in pieces:
+            c += T.upsert_dev(u, b_.data_ptr(), o_.data_ptr(), n_, kache.KEEP, 0, 0)
+        ins["n"] = c
+
+    ms = timed_steps(stream, step, args.steps, args.warmup)
+    T.profile(True)
+    step()
+    torch.cuda.synchronize()
+    rz_ms, rz_n = T.profile_read(4)
+    up_ms, up_n = T.profile_read(0)
+    T.profile(False)
+    size, cap = T.size(), T.capacity()
+    T.close()
+    t_ref, threads = ref_sample(6, 1_000_000, 0.8, False, [("ref_bench_upsert", bs, (0, 0))])
+    cpu = None if t_ref is None else {"value": P / t_ref, "unit": "k-mers/s", "cores": threads, "kind": "reference",
+                                      "sample": "the whole stream once, batches of 64 pieces over the threads"}
+    config_line("k-mers/s insert (config 4: <32,set,20> n=1M, doubling as it fills)", P / (ms * 1e-3), ms,
+                {"workload": f"config 4 at scale {args.scale}: {len(g)} bp genome as {bs.n} pieces of 150 bp, calls of 65,536 pieces",
+                 "positions": P, "inserted": ins["n"], "keys": size, "capacity": cap},
+                cpu=cpu, extra={"profile_one_step": {"insert_ms": up_ms, "insert_launches": up_n, "rebuild_ms": rz_ms,
+                                                     "rebuild_launches": rz_n}})
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=30)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--config", type=int, default=1, choices=[1, 2, 3, 4],
+                    help="the workload: 1 (the headline line), or one of the other configurations, printed for the record")
+    ap.add_argument("--scale", type=float, default=1.0, help="size of configurations 2-4 relative to their full size")
     ap.add_argument("--only-dev", action="store_true",
                     help="time the device-resident steps only (no e2e, CPU baseline or clock sampling): the profiling case")
     args = ap.parse_args()
-    if args.impl == "reference":
+    if args.config != 1:
+        {2: run_config2, 3: run_config3, 4: run_config4}[args.config](args)
+    elif args.impl == "reference":
         run_reference(args)
     else:
         run_b200(args)

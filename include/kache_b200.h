@@ -84,8 +84,8 @@ uint64_t kache_b200_kernel_launches(void) KACHE_NOEXCEPT;
 /* The current device's memory roofs over an array of `bytes` (rounded down to a power of 2; at least 1 MiB), as the
  * reference's roof tool measures the host's (tools/memory-roof.cpp:21-29). kind 0: sequential reads, *rate in
  * bytes/s; 1: independent random reads of 32-byte sectors, *rate in sectors/s; 2: independent random atomic adds,
- * one per sector, *rate in updates/s; 3: dependent random reads (a pointer chase over sectors), *rate in loads/s over
- * all threads. `accesses` sets the random kinds' work; *ms is the timed launch's duration. Allocates and frees the
+ * one per sector, *rate in updates/s; 3: dependent random reads (a pointer chase over sectors by one warp per SM, so
+ * nearly unloaded), *rate in loads/s over those threads. `accesses` sets the random kinds' work; *ms is the timed launch's duration. Allocates and frees the
  * array itself. */
 int kache_b200_memory_roof(uint64_t bytes, uint32_t kind, uint64_t accesses, double* ms, double* rate) KACHE_NOEXCEPT;
 

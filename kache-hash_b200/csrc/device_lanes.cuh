@@ -28,8 +28,10 @@ __global__ void __launch_bounds__(lane_block) lane_kernel(const Dev_Batch batch,
     constexpr uint64_t kmask = (k == 32 ? ~0ull : (1ull << (2 * k)) - 1);
     constexpr uint64_t lmask = (l == 32 ? ~0ull : (1ull << (2 * l)) - 1);
     __shared__ uint64_t blk[w][lane_block];     // This thread's column: the current block's l-mer hashes, then suffix minima.
+    __shared__ uint4 csc[2][lane_block];        // This thread's copy of its last primary bucket's checksums.
     const uint32_t lane = threadIdx.x & 31;
     vis.begin();
+    vis.lane_cache(&csc[0][threadIdx.x], &csc[1][threadIdx.x]);
 
     const uint64_t stride = uint64_t(gridDim.x) * lane_block;
     for(uint64_t g0 = seg_b + uint64_t(blockIdx.x) * lane_block + (threadIdx.x & ~31u); g0 < seg_e; g0 += stride)

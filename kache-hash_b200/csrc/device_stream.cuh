@@ -203,7 +203,10 @@ struct Upsert_Visitor
     const unsigned int* retry_in;
     unsigned int* retried;      // Set to 1 if any bit of retry_out was set.
     unsigned long long ins;
+    Bucket_Cache bc;            // Bound by the lane kernel; unbound (lo null) elsewhere.
     static constexpr int stage_bytes = 0;
+
+    __device__ __forceinline__ void lane_cache(uint4* lo, uint4* hi) { bc.lo = lo, bc.hi = hi, bc.b = ~0ull; }
 
     __device__ __forceinline__ void begin() { ins = 0; }
     __device__ __forceinline__ void begin(uint8_t*) { ins = 0; }
@@ -224,7 +227,7 @@ struct Upsert_Visitor
         Landing L{};
         uint32_t r = NONE;
         if(active)
-            r = upsert_chain<set_>(T, d.key, d.h, d.c, L);
+            r = upsert_chain<set_>(T, d.key, d.h, d.c, L, bc.lo ? &bc : nullptr);
         const bool comm = fn.commutes();
         if(r == INSERTED)
         {
@@ -268,7 +271,10 @@ struct Update_Visitor
     Fn fn;
     unsigned long long* present;
     unsigned long long cnt;
+    Bucket_Cache bc;            // Bound by the lane kernel (exact: an update inserts nothing); unbound elsewhere.
     static constexpr int stage_bytes = 0;
+
+    __device__ __forceinline__ void lane_cache(uint4* lo, uint4* hi) { bc.lo = lo, bc.hi = hi, bc.b = ~0ull; }
 
     __device__ __forceinline__ void begin() { cnt = 0; }
     __device__ __forceinline__ void begin(uint8_t*) { cnt = 0; }
@@ -281,7 +287,7 @@ struct Update_Visitor
     {
         unsigned long long* v = nullptr;
         if(d.valid)
-            v = find_chain<false, true>(T, d.key, d.h, d.c);
+            v = find_chain<false, true>(T, d.key, d.h, d.c, bc.lo ? &bc : nullptr);
         if(v)
             fn.apply(v, d.fwd);
         cnt += __popc(__ballot_sync(0xFFFFFFFFu, v != nullptr));
@@ -308,6 +314,7 @@ struct Lookup_Visitor
     __device__ __forceinline__ void lane_begin(const uint64_t q, const bool has) { obase = has ? pos_off[q] : 0; }
     __device__ __forceinline__ void lane_end(uint64_t, bool) {}
     __device__ __forceinline__ void end(uint32_t) {}
+    __device__ __forceinline__ void lane_cache(uint4*, uint4*) {}
 
     __device__ __forceinline__ void visit(const Kmer_Desc& d, const uint32_t)
     {
@@ -337,7 +344,10 @@ struct Seq_Reduce_Visitor
     V m_fwd, m_rev;
     unsigned long long acc;
     unsigned long long total;
+    Bucket_Cache bc;
     static constexpr int stage_bytes = 0;
+
+    __device__ __forceinline__ void lane_cache(uint4* lo, uint4* hi) { bc.lo = lo, bc.hi = hi, bc.b = ~0ull; }
 
     __device__ __forceinline__ void begin() { total = 0; }
     __device__ __forceinline__ void begin(uint8_t*) { total = 0; }
@@ -347,7 +357,7 @@ struct Seq_Reduce_Visitor
         if(!d.valid)
             return;
         unsigned long long w = 0;
-        if(!find_chain<set_, false>(T, d.key, d.h, d.c, w))
+        if(!find_chain<set_, false>(T, d.key, d.h, d.c, w, bc.lo ? &bc : nullptr))
             return;
         if constexpr(mode_ == 0)
             acc += 1;
@@ -394,6 +404,7 @@ struct Describe_Visitor
     __device__ __forceinline__ void end_segment(uint64_t, uint32_t) {}
     __device__ __forceinline__ void lane_begin(uint64_t, bool) {}
     __device__ __forceinline__ void lane_end(uint64_t, bool) {}
+    __device__ __forceinline__ void lane_cache(uint4*, uint4*) {}
     __device__ __forceinline__ void end(uint32_t) {}
     __device__ __forceinline__ void visit(const Kmer_Desc& d, const uint32_t)
     {

@@ -244,13 +244,56 @@ __device__ __forceinline__ unsigned long long* key_word(const Dev_Table& T, cons
     return T.slots + (b * B + j) * slot_words<set_>();
 }
 
+// A lane's copy, in shared memory, of the checksums of the last primary bucket it probed: consecutive k-mers of a
+// read mostly share their minimizer, so their primary bucket, and the copy saves re-reading its sector. The copy may
+// miss checksums published since by other lanes. Every probe stays correct with such a copy, only slower: a missed
+// candidate of an upsert is met by the claim scan's failed compare-and-swap, whose result is the claimer's key, and
+// finds and updates run in kernels without inserts, where nothing changes.
+struct Bucket_Cache
+{
+    uint4* lo;      // Checksums of slots 0..15 and 16..31.
+    uint4* hi;
+    uint64_t b;     // The bucket copied; ~0 for none.
+};
+
+// The checksums of bucket b, from the cache where it holds them, else loaded (and cached).
+template <bool cg_>
+__device__ __forceinline__ void bucket_cs(const Dev_Table& T, const uint64_t b, Bucket_Cache* bc, uint4& c0, uint4& c1)
+{
+    if(bc && bc->b == b)
+    {
+        c0 = *bc->lo, c1 = *bc->hi;
+        return;
+    }
+    const uint8_t* csb = T.cs + b * B;
+    c0 = cg_ ? ld_cg4(csb) : *reinterpret_cast<const uint4*>(csb);
+    c1 = cg_ ? ld_cg4(csb + 16) : *reinterpret_cast<const uint4*>(csb + 16);
+    if(bc)
+        *bc->lo = c0, *bc->hi = c1, bc->b = b;
+}
+
 // Tries the bucket b for the key: its published candidates, then the claim scan. Returns FOUND, FOUND_PENDING or
-// INSERTED with the slot at `j`, or NONE if the bucket is full without the key.
+// INSERTED with the slot at `j`, or NONE if the bucket is full without the key. With a cache holding b, the cached
+// candidates are tried first; if none is the key, the checksums are read afresh (other lanes may have published it
+// since), cached, and the probe goes on from them. A slot this lane claims is entered in the cache.
 template <bool set_>
-__device__ __forceinline__ uint32_t bucket_upsert(const Dev_Table& T, const uint64_t b, const unsigned long long key_st, const uint8_t c, uint32_t& j_out)
+__device__ __forceinline__ uint32_t bucket_upsert(const Dev_Table& T, const uint64_t b, const unsigned long long key_st, const uint8_t c, uint32_t& j_out, Bucket_Cache* bc = nullptr)
 {
     const uint8_t* csb = T.cs + b * B;
-    const uint4 c0 = ld_cg4(csb), c1 = ld_cg4(csb + 16);
+    uint4 c0, c1;
+    if(bc && bc->b == b)
+    {
+        c0 = *bc->lo, c1 = *bc->hi;
+        for(uint32_t cand = candidates32<true>(c0, c1, c); cand; cand &= cand - 1)
+        {
+            const uint32_t j = candidate_slot(__ffs(cand) - 1);
+            if(ld_cg(key_word<set_>(T, b, j)) == key_st)
+                return j_out = j, FOUND;
+        }
+    }
+    c0 = ld_cg4(csb), c1 = ld_cg4(csb + 16);
+    if(bc)
+        *bc->lo = c0, *bc->hi = c1, bc->b = b;
     uint32_t cand = candidates32<true>(c0, c1, c);
     while(cand)
     {
@@ -268,7 +311,11 @@ __device__ __forceinline__ uint32_t bucket_upsert(const Dev_Table& T, const uint
         unsigned long long* kw = key_word<set_>(T, b, j);
         const unsigned long long cur = atomicCAS(kw, 0ull, key_st);
         if(cur == 0)
+        {
+            if(bc)
+                reinterpret_cast<uint8_t*>(j < 16 ? bc->lo : bc->hi)[j & 15] = c;
             return j_out = j, INSERTED;
+        }
         if(cur == key_st)
             return j_out = j, (ld_volatile_u8(csb + j) != 0 ? FOUND : FOUND_PENDING);
     }
@@ -309,12 +356,12 @@ struct Landing
 // The upsert chain of one k-mer (include/Streaming_Kmer_Hash_Table.hpp:2431-2490, lock-free): primary bucket; if
 // full, mark its spill filter, then the secondary buckets in order; then the overflow table.
 template <bool set_>
-__device__ __forceinline__ uint32_t upsert_chain(const Dev_Table& T, const uint64_t key, const uint64_t h, const uint8_t c, Landing& L)
+__device__ __forceinline__ uint32_t upsert_chain(const Dev_Table& T, const uint64_t key, const uint64_t h, const uint8_t c, Landing& L, Bucket_Cache* bc = nullptr)
 {
     const unsigned long long key_st = ~key;
     uint32_t j;
     const uint64_t b = bucket_of(h, T.cap);
-    uint32_t r = bucket_upsert<set_>(T, b, key_st, c, j);
+    uint32_t r = bucket_upsert<set_>(T, b, key_st, c, j, bc);
     uint64_t at = b;
     if(r == NONE)
     {
@@ -377,7 +424,7 @@ __device__ __forceinline__ bool await_published(const Landing& L)
 // Returns the value word (the key word for a set), or null if absent; a map's value word, read together with its key
 // in one 16-byte load, also goes to `val`.
 template <bool set_, bool cg_>
-__device__ __forceinline__ unsigned long long* find_chain(const Dev_Table& T, const uint64_t key, const uint64_t h, const uint8_t c, unsigned long long& val)
+__device__ __forceinline__ unsigned long long* find_chain(const Dev_Table& T, const uint64_t key, const uint64_t h, const uint8_t c, unsigned long long& val, Bucket_Cache* bc = nullptr)
 {
     const unsigned long long key_st = ~key;
     // Compares the key of the slot at kw (16-byte aligned for a map), keeping its value.
@@ -392,11 +439,10 @@ __device__ __forceinline__ unsigned long long* find_chain(const Dev_Table& T, co
             return s.x == key_st;
         }
     };
-    const auto probe = [&](const uint64_t b, bool& full) -> unsigned long long*
+    const auto probe = [&](const uint64_t b, bool& full, Bucket_Cache* pc) -> unsigned long long*
     {
-        const uint8_t* csb = T.cs + b * B;
-        const uint4 c0 = cg_ ? ld_cg4(csb) : *reinterpret_cast<const uint4*>(csb);
-        const uint4 c1 = cg_ ? ld_cg4(csb + 16) : *reinterpret_cast<const uint4*>(csb + 16);
+        uint4 c0, c1;
+        bucket_cs<cg_>(T, b, pc, c0, c1);
         uint32_t cand = candidates32<false>(c0, c1, c);
         while(cand)
         {
@@ -412,7 +458,7 @@ __device__ __forceinline__ unsigned long long* find_chain(const Dev_Table& T, co
 
     const uint64_t b = bucket_of(h, T.cap);
     bool full = false;
-    if(auto* r = probe(b, full))
+    if(auto* r = probe(b, full, bc))
         return r;
     if(!full)
         return nullptr;
@@ -424,9 +470,9 @@ __device__ __forceinline__ unsigned long long* find_chain(const Dev_Table& T, co
     uint64_t p, q;
     secondaries(h, T.cap, p, q);
     bool full_p = false, full_q = false;
-    if(auto* r = probe(p, full_p))
+    if(auto* r = probe(p, full_p, nullptr))
         return r;
-    if(auto* r = probe(q, full_q))
+    if(auto* r = probe(q, full_q, nullptr))
         return r;
     if(!(full_p && full_q))
         return nullptr;
@@ -445,10 +491,10 @@ __device__ __forceinline__ unsigned long long* find_chain(const Dev_Table& T, co
 }
 
 template <bool set_, bool cg_>
-__device__ __forceinline__ unsigned long long* find_chain(const Dev_Table& T, const uint64_t key, const uint64_t h, const uint8_t c)
+__device__ __forceinline__ unsigned long long* find_chain(const Dev_Table& T, const uint64_t key, const uint64_t h, const uint8_t c, Bucket_Cache* bc = nullptr)
 {
     unsigned long long val;
-    return find_chain<set_, cg_>(T, key, h, c, val);
+    return find_chain<set_, cg_>(T, key, h, c, val, bc);
 }
 
 // The value of a found key, as read with it.

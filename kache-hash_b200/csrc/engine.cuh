@@ -486,13 +486,23 @@ class Engine final : public kache_table
 
     // Stages a host batch: offsets, positions and segments computed here, bases gathered into pinned memory and copied
     // in pieces, each piece's H2D copy running while the next one is gathered.
-    // Positions per segment: short segments for the lane kernel (many lanes per batch), 512 for the warp kernel (16
-    // rows per warp); eight times longer while a sequence would have more segments than a list entry indexes.
-    static uint32_t first_seg_len(const bool lanes) { return lanes ? lane_seg_positions : seg_positions; }
-
-    static uint32_t seg_len_for(const bool lanes, const uint64_t max_pos)
+    // Positions per segment: 512 for the warp kernel (16 rows per warp); for the lane kernel 64, or down to 16 in a
+    // batch too small to give each of the GPU's threads 64 positions, so that small batches still spread over every
+    // SM; eight times longer while a sequence would have more segments than a list entry indexes.
+    uint32_t first_seg_len(const bool lanes, const uint64_t total_pos) const
     {
-        uint64_t s = first_seg_len(lanes);
+        if(!lanes)
+            return seg_positions;
+        const uint64_t threads = uint64_t(sm_count_) * 2048;
+        uint32_t s = lane_seg_positions;
+        while(s > 16 && total_pos < uint64_t(s) * threads)
+            s /= 2;
+        return s;
+    }
+
+    uint32_t seg_len_for(const bool lanes, const uint64_t max_pos, const uint64_t total_pos) const
+    {
+        uint64_t s = first_seg_len(lanes, total_pos);
         while((max_pos + s - 1) / s > max_seg_index + 1)
             s *= 8;
         return static_cast<uint32_t>(s);
@@ -500,18 +510,19 @@ class Engine final : public kache_table
 
     Batch_Info stage_host(const char* const* seqs, const size_t* lens, const size_t n, const bool lanes)
     {
-        uint64_t bytes = 0, max_pos = 0;
+        uint64_t bytes = 0, max_pos = 0, all_pos = 0;
         bool contiguous = true;
         for(size_t i = 0; i < n; ++i)
         {
             bytes += lens[i];
-            max_pos = std::max<uint64_t>(max_pos, lens[i] >= size_t(k) ? lens[i] - k + 1 : 0);
+            const uint64_t np = lens[i] >= size_t(k) ? lens[i] - k + 1 : 0;
+            max_pos = std::max<uint64_t>(max_pos, np), all_pos += np;
             if(i + 1 < n && seqs[i] + lens[i] != seqs[i + 1])
                 contiguous = false;
         }
         // Sequences laid end to end in page-locked memory are copied to the device as they lie, with no gather.
         const bool direct = n > 0 && bytes > 0 && contiguous && pinned(seqs[0]) && pinned(seqs[0] + bytes - 1);
-        const uint32_t seg_len = seg_len_for(lanes, max_pos);
+        const uint32_t seg_len = seg_len_for(lanes, max_pos, all_pos);
         uint64_t nsegs = 0;
         for(size_t i = 0; i < n; ++i)
         {
@@ -593,7 +604,8 @@ class Engine final : public kache_table
         auto* seg_off = reinterpret_cast<uint64_t*>(d + o_sego);
         unsigned int* too_long = reinterpret_cast<unsigned int*>(ctr() + 3);
         uint64_t* h = pin_ctr_.as<uint64_t>(32);
-        uint32_t seg_len = first_seg_len(lanes);
+        uint32_t seg_len = first_seg_len(lanes, ~0ull);
+        bool sized = false;     // Whether the lane segments were fitted to the batch's positions.
         for(;;)
         {
             check(cudaMemsetAsync(too_long, 0, 4, stream_), "memset");
@@ -613,9 +625,19 @@ class Engine final : public kache_table
             check(cudaMemcpyAsync(h + 1, seg_off + n, 8, cudaMemcpyDeviceToHost, stream_), "D2H");
             check(cudaMemcpyAsync(h + 2, too_long, 4, cudaMemcpyDeviceToHost, stream_), "D2H");
             sync();
-            if(!static_cast<uint32_t>(h[2]))
-                break;
-            seg_len *= 8;   // A sequence has more segments than a list entry indexes.
+            if(static_cast<uint32_t>(h[2]))
+            {
+                seg_len *= 8;   // A sequence has more segments than a list entry indexes.
+                sized = true;
+                continue;
+            }
+            if(!sized && first_seg_len(lanes, h[0]) < seg_len)
+            {
+                seg_len = first_seg_len(lanes, h[0]);   // A small batch: count again with shorter segments.
+                sized = true;
+                continue;
+            }
+            break;
         }
         const uint64_t total_pos = h[0], nsegs = h[1];
         dbatch_.ensure(nsegs * 8 + 8);

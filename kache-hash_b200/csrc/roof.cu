@@ -47,13 +47,14 @@ __global__ void __launch_bounds__(roof_block) roof_random(uint4* a, const uint64
             s[u] = splitmix64(seed ^ (t * per + i + u)) & mask;
         if constexpr(kind_ == 1)
         {
-            uint4 v[roof_unroll][2];
+            // One 16-byte load per sector: HBM moves the whole 32-byte sector either way.
+            uint4 v[roof_unroll];
 #pragma unroll
             for(int u = 0; u < roof_unroll; ++u)
-                v[u][0] = __ldcg(a + 2 * s[u]), v[u][1] = __ldcg(a + 2 * s[u] + 1);
+                v[u] = __ldcg(a + 2 * s[u]);
 #pragma unroll
             for(int u = 0; u < roof_unroll; ++u)
-                acc ^= v[u][0].x ^ v[u][1].w;
+                acc ^= v[u].x ^ v[u].w;
         }
         else
         {
@@ -76,7 +77,7 @@ __global__ void roof_chase_init(uint4* a, const uint64_t sectors, const uint64_t
 
 __global__ void __launch_bounds__(roof_block) roof_chase(const uint4* a, const uint64_t mask, const uint32_t per, unsigned long long* sink)
 {
-    const uint64_t t = uint64_t(blockIdx.x) * roof_block + threadIdx.x;
+    const uint64_t t = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x;
     uint64_t s = splitmix64(t) & mask;
     for(uint32_t i = 0; i < per; ++i)
         s = __ldcg(reinterpret_cast<const unsigned long long*>(a + 2 * s)) & mask;
@@ -111,7 +112,7 @@ extern "C" int kache_b200_memory_roof(const uint64_t bytes, const uint32_t kind,
         check(cudaMemset(a, 0, sectors * 32), "memset");
         check(cudaEventCreate(&e0), "event"), check(cudaEventCreate(&e1), "event");
         const unsigned blocks = static_cast<unsigned>(sms) * 8;    // 2048 threads per SM.
-        const uint64_t threads = uint64_t(blocks) * roof_block;
+        const uint64_t threads = kind == 3 ? uint64_t(sms) * 32 : uint64_t(blocks) * roof_block;
         uint32_t per = static_cast<uint32_t>(std::max<uint64_t>(1, (accesses + threads - 1) / threads));
         if(kind == 1 || kind == 2)
             per = (per + roof_unroll - 1) / roof_unroll * roof_unroll;
@@ -129,7 +130,7 @@ extern "C" int kache_b200_memory_roof(const uint64_t bytes, const uint32_t kind,
             case 0: roof_seq_read<<<blocks, roof_block>>>(a, sectors * 2, sink); break;
             case 1: roof_random<1><<<blocks, roof_block>>>(a, mask, per, 0x2545F4914F6CDD1Dull + rep, sink); break;
             case 2: roof_random<2><<<blocks, roof_block>>>(a, mask, per, 0x2545F4914F6CDD1Dull + rep, sink); break;
-            default: roof_chase<<<blocks, roof_block>>>(a, mask, per, sink); break;
+            default: roof_chase<<<static_cast<unsigned>(sms), 32>>>(a, mask, per, sink); break;  // A warp per SM: the unloaded latency.
             }
             launches()++;
             check(cudaGetLastError(), "launch");
@@ -139,7 +140,7 @@ extern "C" int kache_b200_memory_roof(const uint64_t bytes, const uint32_t kind,
         }
         *ms = t;
         // Sequential: bytes per second. Random reads and updates: sectors per second. Chase: dependent loads per
-        // second over all threads (the latency is threads / rate).
+        // second of one warp per SM (the latency is those threads / rate).
         const double done = kind == 0 ? static_cast<double>(sectors * 32) : static_cast<double>(threads) * per;
         *rate = done / (t * 1e-3);
     }

@@ -294,6 +294,16 @@ class Table:
         _check(lib().kache_b200_upsert_dev(self.h, user, d_bases, d_off, n, op, x, init, ctypes.byref(r)), "upsert_dev")
         return r.value
 
+    def upsert_oriented_dev(self, user, d_bases, d_off, n, op, x_fwd, x_rev):
+        r = ctypes.c_uint64()
+        _check(lib().kache_b200_upsert_oriented_dev(self.h, user, d_bases, d_off, n, op, x_fwd, x_rev, ctypes.byref(r)), "upsert_oriented_dev")
+        return r.value
+
+    def update_dev(self, d_bases, d_off, n, op, x):
+        r = ctypes.c_uint64()
+        _check(lib().kache_b200_update_dev(self.h, d_bases, d_off, n, op, x, ctypes.byref(r)), "update_dev")
+        return r.value
+
     def lookup_dev(self, d_bases, d_off, n, d_found, d_values=None, d_fwd=None):
         _check(lib().kache_b200_lookup_dev(self.h, d_bases, d_off, n, d_found, d_values, d_fwd), "lookup_dev")
 

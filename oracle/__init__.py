@@ -217,6 +217,8 @@ def ref():
             "ref_dump": (_u64, [_vp, _vp, _vp]),
             "ref_bench_upsert": (ctypes.c_double, [_vp, _vp, _vp, _u64, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32, _u64, ctypes.POINTER(_u64)]),
             "ref_bench_count": (ctypes.c_double, [_vp, _vp, _vp, _u64, ctypes.c_uint32, ctypes.c_uint32, ctypes.POINTER(_u64)]),
+            "ref_bench_upsert_oriented": (ctypes.c_double, [_vp, _vp, _vp, _u64, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32, _u64, _u64, ctypes.POINTER(_u64)]),
+            "ref_bench_update": (ctypes.c_double, [_vp, _vp, _vp, _u64, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32, _u64, ctypes.POINTER(_u64)]),
             "ref_bench_lookup": (ctypes.c_double, [_vp, _vp, _vp, _u64, _vp, ctypes.c_uint32, ctypes.c_uint32, _vp, _vp]),
         }
         for name, (res, args) in sig.items():

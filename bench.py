@@ -651,20 +651,120 @@ def run_config4(args):
                                                      "rebuild_launches": rz_n}})
 
 
+def run_config5(args):
+    """Served mixed requests (upsert ADD 1 / find / count at 60/30/10) on a <31, u32, 22> map primed with a genome's
+    31-mers: the same requests run one by one through the plain calls, then through the request server submitted at
+    once from four client threads (throughput), then through the server at Poisson arrivals at 60 % of that
+    throughput (latency)."""
+    import threading
+    import torch
+    import kache
+    from kache import Batch
+    dev = torch.device("cuda", 0)
+    rng = np.random.default_rng(53)
+    glen = int(2_000_000_000 * args.scale)
+    g = synth.genome(glen, seed=51)
+    T = kache.Table(31, 4, glen, 0.8, False)
+    u = T.register()
+    ib, io, ni = dev_batch(Batch(*synth.stretches(g, 1_000_000)), dev)
+    T.upsert_dev(u, ib.data_ptr(), io.data_ptr(), ni, kache.KEEP, 0, 0)
+    torch.cuda.synchronize()
+    primed = T.size()
+    del ib, io
+    pool = Batch(*synth.reads_fixed(g, min(4_000_000, max(100_000, glen // 100)), 150, seed=52, sub=0.01, n_rate=0.0005))
+    reqs = []
+    for _ in range(args.requests):
+        kind = rng.choice(3, p=[0.6, 0.3, 0.1])
+        m = int(np.clip(rng.lognormal(np.log(2000), 1.5), 1, min(1_000_000, pool.n)))
+        s = int(rng.integers(0, pool.n - m + 1))
+        reqs.append((int(kind), pool.slice(s, s + m)))
+    P = sum(int(b.positions(31).sum()) for _, b in reqs)
+
+    def outputs(kind, b):
+        p = int(b.positions(31).sum())
+        if kind == 1:
+            return np.zeros(max(p, 1), np.uint8), np.zeros(max(p, 1), np.uint32), None
+        if kind == 2:
+            return np.zeros(max(b.n, 1), np.uint64), None, None
+        return None, None, None
+
+    # Plain: one call per request, in order.
+    t0 = time.perf_counter()
+    for kind, b in reqs:
+        if kind == 0:
+            T.upsert(u, b, kache.ADD, 1, 1)
+        elif kind == 1:
+            T.lookup(b, values=True, fwd=False)
+        else:
+            T.count(b)
+    plain_s = time.perf_counter() - t0
+
+    S = kache.Server(T)
+
+    def serve(arrivals):
+        """Submits request i at arrivals[i] seconds (all at once if None) from four threads; returns wall seconds and
+        latencies."""
+        tickets = [None] * len(reqs)
+        outs = [outputs(kind, b) for kind, b in reqs]
+        start = time.perf_counter()
+
+        def client(idx):
+            for i in idx:
+                if arrivals is not None:
+                    delay = start + arrivals[i] - time.perf_counter()
+                    if delay > 0:
+                        time.sleep(delay)
+                kind, b = reqs[i]
+                o = outs[i]
+                tickets[i] = S.submit(kind, b, op=kache.ADD, x=1, init=1, out0=o[0], out1=o[1], out2=o[2])
+
+        th = [threading.Thread(target=client, args=(range(j, len(reqs), 4),)) for j in range(4)]
+        for t in th:
+            t.start()
+        for t in th:
+            t.join()
+        lat = [S.wait(t)[1] for t in tickets]
+        return time.perf_counter() - start, np.array(lat)
+
+    runs0, _ = S.stats()
+    burst_s, burst_lat = serve(None)
+    runs1, _ = S.stats()
+    rate = 0.6 * len(reqs) / burst_s
+    arrivals = np.cumsum(rng.exponential(1.0 / rate, size=len(reqs)))
+    open_s, open_lat = serve(arrivals)
+    runs2, _ = S.stats()
+    S.close()
+    st = T.stats()
+    T.close()
+    pct = lambda a, q: float(np.percentile(a, q))
+    config_line("k-mers/s served mix (config 5: <31,u32,22> primed map, upsert ADD 1 / find / count at 60/30/10)",
+                P / burst_s, 1000 * burst_s,
+                {"workload": f"config 5 at scale {args.scale}: {glen} bp genome primed ({primed} keys); {len(reqs)} requests of "
+                             "150 bp reads (1% errors), lognormal(2000, 1.5) reads each, clipped 1-1M",
+                 "positions": P, "keys_after": st.keys, "capacity_after": st.capacity},
+                extra={"plain": {"value": P / plain_s, "ms": 1000 * plain_s, "calls": len(reqs)},
+                       "served_burst": {"value": P / burst_s, "p50_ms": pct(burst_lat, 50), "p99_ms": pct(burst_lat, 99),
+                                        "runs": runs1 - runs0, "requests": len(reqs)},
+                       "served_poisson": {"offered_requests_per_s": rate, "value": P / open_s, "p50_ms": pct(open_lat, 50),
+                                          "p99_ms": pct(open_lat, 99), "runs": runs2 - runs1},
+                       "host_buffers": "pageable (the library stages them)"})
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=30)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--config", type=int, default=1, choices=[1, 2, 3, 4],
+    ap.add_argument("--config", type=int, default=1, choices=[1, 2, 3, 4, 5],
                     help="the workload: 1 (the headline line), or one of the other configurations, printed for the record")
-    ap.add_argument("--scale", type=float, default=1.0, help="size of configurations 2-4 relative to their full size")
+    ap.add_argument("--scale", type=float, default=1.0, help="size of configurations 2-5 relative to their full size")
+    ap.add_argument("--requests", type=int, default=300, help="requests of configuration 5")
     ap.add_argument("--only-dev", action="store_true",
                     help="time the device-resident steps only (no e2e, CPU baseline or clock sampling): the profiling case")
     args = ap.parse_args()
     if args.config != 1:
-        {2: run_config2, 3: run_config3, 4: run_config4}[args.config](args)
+        {2: run_config2, 3: run_config3, 4: run_config4, 5: run_config5}[args.config](args)
     elif args.impl == "reference":
         run_reference(args)
     else:

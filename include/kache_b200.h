@@ -89,6 +89,27 @@ uint64_t kache_b200_kernel_launches(void) KACHE_NOEXCEPT;
  * array itself. */
 int kache_b200_memory_roof(uint64_t bytes, uint32_t kind, uint64_t accesses, double* ms, double* rate) KACHE_NOEXCEPT;
 
+/* A request server over a table (no counterpart in the reference, whose callers share a table through user tokens):
+ * requests submitted from any threads are run by one dispatcher thread, which merges the requests waiting when the
+ * GPU frees up into one call: the oldest waiting request and all waiting requests of its kind (and, for upserts,
+ * the same op, x and init) whose staging fits `budget_bytes` (0: no limit beyond half the device memory free at
+ * creation). Requests of one kind run in submission order; waiting requests of different kinds are concurrent (wait
+ * for a request before submitting one that must see it). Runs never overlap, so queries never overlap inserts. A request's sequences and output arrays must stay valid until
+ * kache_b200_server_wait returns for it. Results: an upsert's keys inserted; a lookup's found flags, values and
+ * orientations as kache_lookup lays them out, and its present positions; a count's per-sequence counts as kache_count
+ * lays them out, and their sum. The server registers one user of the table. */
+typedef struct kache_server kache_server;
+#define KACHE_B200_REQ_UPSERT 0u   /* op, x, init as kache_b200_upsert; out0..2 unused */
+#define KACHE_B200_REQ_LOOKUP 1u   /* out0 found (required), out1 values (or NULL), out2 fwd (or NULL) */
+#define KACHE_B200_REQ_COUNT  2u   /* out0 counts, uint64_t per sequence */
+int kache_b200_server_new(kache_table* t, uint64_t budget_bytes, kache_server** out) KACHE_NOEXCEPT;
+void kache_b200_server_free(kache_server* s) KACHE_NOEXCEPT;
+int kache_b200_server_submit(kache_server* s, uint32_t kind, const char* const* seqs, const size_t* lens, size_t n, uint32_t op, uint64_t x, uint64_t init, void* out0, void* out1, void* out2, uint64_t* ticket) KACHE_NOEXCEPT;
+/* Waits for a request; its result at *result, the time from its submission to its completion at *latency_ms. */
+int kache_b200_server_wait(kache_server* s, uint64_t ticket, uint64_t* result, double* latency_ms) KACHE_NOEXCEPT;
+/* Merged runs so far, and the requests they ran. */
+int kache_b200_server_stats(kache_server* s, uint64_t* runs, uint64_t* requests) KACHE_NOEXCEPT;
+
 /* Reads the FASTA or FASTQ file (or pipe) at `path` and calls f(ctx, seqs, lens, n) with its non-empty sequences in
  * order, in batches of whole sequences of about `batch_bases` bases, until f returns nonzero
  * (counter/Fastx_Reader.hpp:13-52). Unreadable, gzip-compressed or malformed input returns KACHE_EINVAL. */

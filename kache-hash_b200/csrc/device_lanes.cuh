@@ -10,7 +10,8 @@
 //
 // Lanes of a warp work on 32 different segments -- for short reads, 32 different reads -- so their inserts rarely
 // meet in one bucket. A warp steps as long as its longest segment; the host lists segments so that neighbours have
-// similar lengths.
+// similar lengths. Warps take their next 32 segments from a work counter (`next`, zeroed before the launch), so warps
+// that drew short segments or fast probes take more, and the launch ends evenly however uneven the reads are.
 #pragma once
 
 #include "device_stream.cuh"
@@ -21,7 +22,7 @@ namespace kache_b200
 constexpr int lane_block = 256;     // Threads per block of the lane kernel.
 
 template <int k, int l, typename Visitor>
-__global__ void __launch_bounds__(lane_block) lane_kernel(const Dev_Batch batch, const uint64_t seg_b, const uint64_t seg_e, Visitor vis)
+__global__ void __launch_bounds__(lane_block) lane_kernel(const Dev_Batch batch, const uint64_t seg_b, const uint64_t seg_e, unsigned long long* next, Visitor vis)
 {
     constexpr int w = k - l + 1;
     static_assert(k <= 32 && l <= k && w >= 1, "k-mers in a machine word");
@@ -33,8 +34,14 @@ __global__ void __launch_bounds__(lane_block) lane_kernel(const Dev_Batch batch,
     vis.begin();
     vis.lane_cache(&csc[0][threadIdx.x], &csc[1][threadIdx.x]);
 
-    const uint64_t stride = uint64_t(gridDim.x) * lane_block;
-    for(uint64_t g0 = seg_b + uint64_t(blockIdx.x) * lane_block + (threadIdx.x & ~31u); g0 < seg_e; g0 += stride)
+    const auto take = [&]() -> uint64_t
+    {
+        unsigned long long g = 0;
+        if(lane == 0)
+            g = atomicAdd(next, 32ull);
+        return seg_b + __shfl_sync(0xFFFFFFFFu, g, 0);
+    };
+    for(uint64_t g0 = take(); g0 < seg_e; g0 = take())
     {
         const uint64_t g = g0 + lane;
         const bool has = g < seg_e;

@@ -203,17 +203,24 @@ struct Upsert_Visitor
     const unsigned int* retry_in;
     unsigned int* retried;      // Set to 1 if any bit of retry_out was set.
     unsigned long long ins;
-    Bucket_Cache bc;            // Bound by the lane kernel; unbound (lo null) elsewhere.
+    unsigned long long* per_seq;    // If set, keys inserted per sequence are added at per_seq[q] (lane kernel only).
+    uint32_t lane_ins;
     static constexpr int stage_bytes = 0;
 
-    __device__ __forceinline__ void lane_cache(uint4* lo, uint4* hi) { bc.lo = lo, bc.hi = hi, bc.b = ~0ull; }
+    // No checksum cache for inserts: other lanes insert into the same buckets meanwhile, and a stale copy's missed
+    // candidates cost a re-read; measured slower than reading the sector each time (config-1 upsert 1.91 vs 1.74 ms).
+    __device__ __forceinline__ void lane_cache(uint4*, uint4*) {}
 
     __device__ __forceinline__ void begin() { ins = 0; }
     __device__ __forceinline__ void begin(uint8_t*) { ins = 0; }
     __device__ __forceinline__ void begin_segment(uint64_t) {}
     __device__ __forceinline__ void end_segment(uint64_t, uint32_t) {}
-    __device__ __forceinline__ void lane_begin(uint64_t, bool) {}
-    __device__ __forceinline__ void lane_end(uint64_t, bool) {}
+    __device__ __forceinline__ void lane_begin(uint64_t, bool) { lane_ins = 0; }
+    __device__ __forceinline__ void lane_end(const uint64_t q, const bool has)
+    {
+        if(per_seq && has && lane_ins)
+            atomicAdd(per_seq + q, static_cast<unsigned long long>(lane_ins));
+    }
 
     __device__ __forceinline__ void visit(const Kmer_Desc& d, const uint32_t lane)
     {
@@ -227,7 +234,7 @@ struct Upsert_Visitor
         Landing L{};
         uint32_t r = NONE;
         if(active)
-            r = upsert_chain<set_>(T, d.key, d.h, d.c, L, bc.lo ? &bc : nullptr);
+            r = upsert_chain<set_>(T, d.key, d.h, d.c, L);
         const bool comm = fn.commutes();
         if(r == INSERTED)
         {
@@ -247,6 +254,7 @@ struct Upsert_Visitor
             *retried = 1;
         }
         ins += __popc(__ballot_sync(0xFFFFFFFFu, r == INSERTED));
+        lane_ins += (r == INSERTED);
         __syncwarp();
 
         if constexpr(!set_)

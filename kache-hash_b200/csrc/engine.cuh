@@ -42,6 +42,8 @@ struct kache_table
 
     virtual void set_stream(cudaStream_t s) = 0;
     virtual uint64_t upsert(uint32_t user, const char* const* seqs, const size_t* lens, size_t n, uint32_t op, uint64_t x, uint64_t init) = 0;
+    // As upsert, also putting the keys each sequence inserted at per_seq[0..n) (host memory).
+    virtual uint64_t upsert_split(uint32_t user, const char* const* seqs, const size_t* lens, size_t n, uint32_t op, uint64_t x, uint64_t init, uint64_t* per_seq) = 0;
     virtual uint64_t upsert_oriented(uint32_t user, const char* const* seqs, const size_t* lens, size_t n, uint32_t op, uint64_t xf, uint64_t xr) = 0;
     virtual uint64_t update(const char* const* seqs, const size_t* lens, size_t n, uint32_t op, uint64_t x) = 0;
     virtual void lookup(const char* const* seqs, const size_t* lens, size_t n, uint8_t* found, void* values, uint8_t* fwd) = 0;
@@ -164,12 +166,14 @@ struct Pinned_Buf
         p = nullptr, bytes = 0;
     }
 
+    // Grows to at least n bytes, at least doubling (page-locking is slow: growing batches reallocate rarely); the
+    // contents are lost on growth.
     void ensure(const size_t n)
     {
         if(n <= bytes)
             return;
+        const size_t m = std::max<size_t>({n + n / 4, 2 * bytes, size_t(1) << 20});
         release();
-        const size_t m = std::max<size_t>(n + n / 4, 1 << 20);
         check(cudaHostAlloc(&p, m, cudaHostAllocDefault), "cudaHostAlloc");
         bytes = m;
     }
@@ -273,6 +277,69 @@ inline bool host_acgt(const char c)
     return x == 'a' || x == 'c' || x == 'g' || x == 't';
 }
 
+// ---- The lane kernel's autotuner ---------------------------------------------------------------------------------
+
+// Picks the lane kernel's segment length -- positions per lane, which sets how many lanes a batch has and how much of
+// each lane's rolling is warm-up -- per operation (upsert, update, per-sequence reduction) and batch size class (the
+// log2 of its positions), online: the first calls of a class try each candidate, in turn from the built-in choice;
+// later calls take the fastest per position (a moving average of the measured kernel time), and every 16th call
+// retries another candidate so the averages follow the table as it fills.
+class Seg_Tuner
+{
+public:
+    static constexpr int cands = 4;
+    static constexpr uint32_t len[cands] = {16, 32, 64, 128};
+
+    // The candidate for a call of `kind` over `pos` positions; `dflt` is the built-in choice.
+    int pick(const int kind, const uint64_t pos, const uint32_t dflt)
+    {
+        Slot& s = slot(kind, pos);
+        int d = 0;
+        while(d + 1 < cands && len[d] < dflt)
+            d++;
+        for(int i = 0; i < cands; ++i)
+        {
+            const int c = (d + i) % cands;
+            if(s.tries[c] == 0)
+                return c;
+        }
+        int best = 0;
+        for(int c = 1; c < cands; ++c)
+            if(s.ns_per_pos[c] < s.ns_per_pos[best])
+                best = c;
+        if(++s.calls % 16 == 0)
+            return (best + 1 + static_cast<int>(s.calls / 16) % (cands - 1)) % cands;
+        return best;
+    }
+
+    void record(const int kind, const uint64_t pos, const int c, const double ms)
+    {
+        if(pos == 0 || c < 0)
+            return;
+        Slot& s = slot(kind, pos);
+        const double v = 1e6 * ms / static_cast<double>(pos);
+        s.ns_per_pos[c] = s.tries[c] == 0 ? v : 0.7 * s.ns_per_pos[c] + 0.3 * v;
+        s.tries[c]++;
+    }
+
+private:
+    struct Slot
+    {
+        double ns_per_pos[cands] = {};
+        uint32_t tries[cands] = {};
+        uint32_t calls = 0;
+    };
+    Slot slots_[3][64];
+
+    Slot& slot(const int kind, const uint64_t pos)
+    {
+        int c = 0;
+        while(c < 63 && (uint64_t(2) << c) <= pos)
+            c++;
+        return slots_[kind][c];
+    }
+};
+
 // ---- The engine --------------------------------------------------------------------------------------------------
 
 enum Kind : uint32_t { K_UPSERT = 0, K_UPDATE = 1, K_LOOKUP = 2, K_REDUCE = 3, K_RESIZE = 4, K_OTHER = 5, K_KINDS = 6 };
@@ -310,6 +377,12 @@ class Engine final : public kache_table
     bool prof_ = false;
     struct Ev { cudaEvent_t a, b; uint32_t kind; };
     std::vector<Ev> ev_;
+    // The autotuner, and the current call's choice and lane-kernel event pairs.
+    Seg_Tuner tuner_;
+    int tune_kind_ = -1, tune_cand_ = -1;
+    uint64_t tune_pos_ = 0;
+    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> tune_ev_;
+    size_t tune_used_ = 0;
     double prof_ms_[K_KINDS] = {};
     uint64_t prof_n_[K_KINDS] = {};
 
@@ -489,10 +562,8 @@ class Engine final : public kache_table
     // Positions per segment: 512 for the warp kernel (16 rows per warp); for the lane kernel 64, or down to 16 in a
     // batch too small to give each of the GPU's threads 64 positions, so that small batches still spread over every
     // SM; eight times longer while a sequence would have more segments than a list entry indexes.
-    uint32_t first_seg_len(const bool lanes, const uint64_t total_pos) const
+    uint32_t builtin_seg_len(const uint64_t total_pos) const
     {
-        if(!lanes)
-            return seg_positions;
         const uint64_t threads = uint64_t(sm_count_) * 2048;
         uint32_t s = lane_seg_positions;
         while(s > 16 && total_pos < uint64_t(s) * threads)
@@ -500,7 +571,40 @@ class Engine final : public kache_table
         return s;
     }
 
-    uint32_t seg_len_for(const bool lanes, const uint64_t max_pos, const uint64_t total_pos) const
+    // The lane segment length for this call: the autotuner's pick for the call's kind, once the batch's positions are
+    // known (total_pos = ~0 while they are not).
+    uint32_t first_seg_len(const bool lanes, const uint64_t total_pos)
+    {
+        if(!lanes)
+            return seg_positions;
+        if(total_pos == ~0ull || tune_kind_ < 0)
+            return builtin_seg_len(total_pos);
+        tune_cand_ = tuner_.pick(tune_kind_, total_pos, builtin_seg_len(total_pos));
+        tune_pos_ = total_pos;
+        return Seg_Tuner::len[tune_cand_];
+    }
+
+    // Starts a tuned call of `kind` (0 upsert, 1 update, 2 per-sequence reduction); finish_tune() records it.
+    void begin_tune(const int kind) { tune_kind_ = kind, tune_cand_ = -1, tune_pos_ = 0, tune_used_ = 0; }
+
+    // After the call's last sync: its lane kernels' time goes to the tuner.
+    void finish_tune()
+    {
+        double ms = 0;
+        for(size_t i = 0; i < tune_used_; ++i)
+        {
+            float t = 0;
+            if(cudaEventElapsedTime(&t, tune_ev_[i].first, tune_ev_[i].second) == cudaSuccess)
+                ms += t;
+            else
+                (void)cudaGetLastError();
+        }
+        if(tune_used_ > 0)
+            tuner_.record(tune_kind_, tune_pos_, tune_cand_, ms);
+        tune_kind_ = -1, tune_cand_ = -1, tune_used_ = 0;
+    }
+
+    uint32_t seg_len_for(const bool lanes, const uint64_t max_pos, const uint64_t total_pos)
     {
         uint64_t s = first_seg_len(lanes, total_pos);
         while((max_pos + s - 1) / s > max_seg_index + 1)
@@ -631,11 +735,15 @@ class Engine final : public kache_table
                 sized = true;
                 continue;
             }
-            if(!sized && first_seg_len(lanes, h[0]) < seg_len)
+            if(!sized && lanes)
             {
-                seg_len = first_seg_len(lanes, h[0]);   // A small batch: count again with shorter segments.
                 sized = true;
-                continue;
+                const uint32_t want = first_seg_len(lanes, h[0]);
+                if(want != seg_len)
+                {
+                    seg_len = want;     // Count again with the segment length chosen for this batch's size.
+                    continue;
+                }
             }
             break;
         }
@@ -663,7 +771,22 @@ class Engine final : public kache_table
             return;
         }
         const uint64_t blocks = std::min<uint64_t>((se - sb + lane_block - 1) / lane_block, uint64_t(sm_count_) * 16);
-        launch(kind, [&](){ lane_kernel<k, l, Vis><<<static_cast<unsigned>(blocks), lane_block, 0, stream_>>>(bi.b, sb, se, vis); });
+        unsigned long long* next = ctr() + 7;     // The lane kernel's work counter.
+        check(cudaMemsetAsync(next, 0, sizeof(unsigned long long), stream_), "memset");
+        const bool timed = tune_kind_ >= 0 && tune_cand_ >= 0;
+        if(timed)
+        {
+            if(tune_used_ == tune_ev_.size())
+            {
+                std::pair<cudaEvent_t, cudaEvent_t> e{};
+                check(cudaEventCreate(&e.first), "event"), check(cudaEventCreate(&e.second), "event");
+                tune_ev_.push_back(e);
+            }
+            check(cudaEventRecord(tune_ev_[tune_used_].first, stream_), "record");
+        }
+        launch(kind, [&](){ lane_kernel<k, l, Vis><<<static_cast<unsigned>(blocks), lane_block, 0, stream_>>>(bi.b, sb, se, next, vis); });
+        if(timed)
+            check(cudaEventRecord(tune_ev_[tune_used_++].second, stream_), "record");
     }
 
     // The reference's per-user flush accounting over one call (include/Streaming_Kmer_Hash_Table.hpp:2248-2286,
@@ -752,7 +875,7 @@ class Engine final : public kache_table
     }
 
     // Upserts a staged batch with the value functor `fn`, chunk by chunk (see the top of this file).
-    template <typename Fn> uint64_t run_upsert(const uint32_t user, const Batch_Info& bi, const Fn& fn)
+    template <typename Fn> uint64_t run_upsert(const uint32_t user, const Batch_Info& bi, const Fn& fn, unsigned long long* per_seq = nullptr)
     {
         const uint64_t nsegs = bi.b.nsegs;
         const double pos_per_seg = nsegs ? static_cast<double>(bi.total_pos) / nsegs : 1.0;
@@ -785,7 +908,7 @@ class Engine final : public kache_table
 
             check(cudaMemsetAsync(ctr(), 0, 8, stream_), "memset");
             check(cudaMemsetAsync(retried, 0, 4, stream_), "memset");
-            Upsert_Visitor<set_, VT, Fn> vis{T_, fn, bi.b.pos_off, ctr(), dretry_a_.as<unsigned int>(), nullptr, retried, 0};
+            Upsert_Visitor<set_, VT, Fn> vis{T_, fn, bi.b.pos_off, ctr(), dretry_a_.as<unsigned int>(), nullptr, retried, 0, per_seq};
             stream_launch(K_UPSERT, bi, sb, se, vis);
             const unsigned long long* c = read_ctr(3);
             uint64_t ins = c[0];
@@ -795,7 +918,7 @@ class Engine final : public kache_table
                 check(cudaMemsetAsync(ctr(), 0, 8, stream_), "memset");
                 check(cudaMemsetAsync(retried, 0, 4, stream_), "memset");
                 check(cudaMemsetAsync(dretry_b_.p, 0, bits, stream_), "memset");
-                Upsert_Visitor<set_, VT, Fn> rv{T_, fn, bi.b.pos_off, ctr(), dretry_b_.as<unsigned int>(), dretry_a_.as<unsigned int>(), retried, 0};
+                Upsert_Visitor<set_, VT, Fn> rv{T_, fn, bi.b.pos_off, ctr(), dretry_b_.as<unsigned int>(), dretry_a_.as<unsigned int>(), retried, 0, per_seq};
                 stream_launch(K_UPSERT, bi, sb, se, rv);
                 check(cudaMemsetAsync(dretry_a_.p, 0, bits, stream_), "memset");
                 std::swap(dretry_a_.p, dretry_b_.p), std::swap(dretry_a_.bytes, dretry_b_.bytes);
@@ -935,6 +1058,8 @@ public:
         for(auto& e : ev_out_)
             if(e)
                 cudaEventDestroy(e);
+        for(auto& e : tune_ev_)
+            cudaEventDestroy(e.first), cudaEventDestroy(e.second);
         if(own_)
             cudaStreamDestroy(own_);
     }
@@ -949,8 +1074,24 @@ public:
     uint64_t upsert(uint32_t user, const char* const* seqs, const size_t* lens, size_t n, uint32_t op, uint64_t x, uint64_t init) override
     {
         std::lock_guard<std::mutex> g(work);
+        begin_tune(0);
         const auto bi = stage_host(seqs, lens, n, true);
-        return run_upsert(user, bi, op_fn(op, x, init));
+        const uint64_t r = run_upsert(user, bi, op_fn(op, x, init));
+        finish_tune();
+        return r;
+    }
+
+    uint64_t upsert_split(uint32_t user, const char* const* seqs, const size_t* lens, size_t n, uint32_t op, uint64_t x, uint64_t init, uint64_t* per_seq) override
+    {
+        std::lock_guard<std::mutex> g(work);
+        begin_tune(0);
+        const auto bi = stage_host(seqs, lens, n, true);
+        dout_.ensure(n * 8 + 8);
+        check(cudaMemsetAsync(dout_.p, 0, n * 8, stream_), "memset");
+        const uint64_t r = run_upsert(user, bi, op_fn(op, x, init), dout_.as<unsigned long long>());
+        d2h(per_seq, dout_.p, n * 8);
+        finish_tune();
+        return r;
     }
 
     uint64_t upsert_oriented(uint32_t user, const char* const* seqs, const size_t* lens, size_t n, uint32_t op, uint64_t xf, uint64_t xr) override
@@ -960,8 +1101,11 @@ public:
         else
         {
             std::lock_guard<std::mutex> g(work);
+            begin_tune(0);
             const auto bi = stage_host(seqs, lens, n, true);
-            return run_upsert(user, bi, Oriented_Op_Fn<VT>{op, static_cast<VT>(xf), static_cast<VT>(xr)});
+            const uint64_t r = run_upsert(user, bi, Oriented_Op_Fn<VT>{op, static_cast<VT>(xf), static_cast<VT>(xr)});
+            finish_tune();
+            return r;
         }
     }
 
@@ -972,8 +1116,11 @@ public:
         else
         {
             std::lock_guard<std::mutex> g(work);
+            begin_tune(1);
             const auto bi = stage_host(seqs, lens, n, true);
-            return run_update(bi, op_fn(op, x, 0));
+            const uint64_t r = run_update(bi, op_fn(op, x, 0));
+            finish_tune();
+            return r;
         }
     }
 
@@ -999,10 +1146,12 @@ public:
     void seq_reduce(const char* const* seqs, const size_t* lens, size_t n, int mode, uint64_t m_fwd, uint64_t m_rev, uint64_t* out) override
     {
         std::lock_guard<std::mutex> g(work);
+        begin_tune(2);
         const auto bi = stage_host(seqs, lens, n, true);
         dout_.ensure(n * 8 + 8);
         run_seq_reduce(bi, mode, m_fwd, m_rev, dout_.as<unsigned long long>());
         d2h(out, dout_.p, n * 8);
+        finish_tune();
     }
 
     void describe(const char* const* seqs, const size_t* lens, size_t n, uint64_t* key, uint64_t* h, uint8_t* cs, uint8_t* fwd, uint8_t* valid) override
@@ -1021,8 +1170,11 @@ public:
     uint64_t upsert_dev(uint32_t user, const uint8_t* b, const uint64_t* off, uint64_t n, uint32_t op, uint64_t x, uint64_t init) override
     {
         std::lock_guard<std::mutex> g(work);
+        begin_tune(0);
         const auto bi = stage_dev(b, off, n, true);
-        return run_upsert(user, bi, op_fn(op, x, init));
+        const uint64_t r = run_upsert(user, bi, op_fn(op, x, init));
+        finish_tune();
+        return r;
     }
 
     uint64_t upsert_oriented_dev(uint32_t user, const uint8_t* b, const uint64_t* off, uint64_t n, uint32_t op, uint64_t xf, uint64_t xr) override
@@ -1032,8 +1184,11 @@ public:
         else
         {
             std::lock_guard<std::mutex> g(work);
+            begin_tune(0);
             const auto bi = stage_dev(b, off, n, true);
-            return run_upsert(user, bi, Oriented_Op_Fn<VT>{op, static_cast<VT>(xf), static_cast<VT>(xr)});
+            const uint64_t r = run_upsert(user, bi, Oriented_Op_Fn<VT>{op, static_cast<VT>(xf), static_cast<VT>(xr)});
+            finish_tune();
+            return r;
         }
     }
 
@@ -1044,8 +1199,11 @@ public:
         else
         {
             std::lock_guard<std::mutex> g(work);
+            begin_tune(1);
             const auto bi = stage_dev(b, off, n, true);
-            return run_update(bi, op_fn(op, x, 0));
+            const uint64_t r = run_update(bi, op_fn(op, x, 0));
+            finish_tune();
+            return r;
         }
     }
 
@@ -1060,9 +1218,11 @@ public:
     void count_dev(const uint8_t* b, const uint64_t* off, uint64_t n, uint64_t* counts) override
     {
         std::lock_guard<std::mutex> g(work);
+        begin_tune(2);
         const auto bi = stage_dev(b, off, n, true);
         run_seq_reduce(bi, 0, 0, 0, reinterpret_cast<unsigned long long*>(counts));
         sync();
+        finish_tune();
     }
 
     bool get(const char* kmer, uint64_t& value) override
@@ -1182,15 +1342,21 @@ public:
     template <typename Fn> uint64_t upsert_with(const uint32_t user, const char* const* seqs, const size_t* lens, const size_t n, const Fn& fn)
     {
         std::lock_guard<std::mutex> g(work);
+        begin_tune(0);
         const auto bi = stage_host(seqs, lens, n, true);
-        return run_upsert(user, bi, fn);
+        const uint64_t r = run_upsert(user, bi, fn);
+        finish_tune();
+        return r;
     }
 
     template <typename Fn> uint64_t update_with(const char* const* seqs, const size_t* lens, const size_t n, const Fn& fn)
     {
         std::lock_guard<std::mutex> g(work);
+        begin_tune(1);
         const auto bi = stage_host(seqs, lens, n, true);
-        return run_update(bi, fn);
+        const uint64_t r = run_update(bi, fn);
+        finish_tune();
+        return r;
     }
 
     Dev_Table device_table() const override { return T_; }

@@ -1,0 +1,329 @@
+// A request server over one table: callers submit upsert, lookup and count requests from any thread as they arrive;
+// one dispatcher thread runs them on the GPU, merging the requests that are waiting when the GPU frees up into one
+// launch (continuous batching): the oldest waiting request and every other waiting request of its kind (and, for
+// upserts, its operation) become a single call over all their sequences, and each request gets its own share of the
+// results back. Requests of one kind run in the order they were submitted; waiting requests of different kinds are
+// concurrent, as the reference's users are, and a caller that needs one to see another waits for the first before
+// submitting the second. Runs of different kinds never overlap, which keeps the reference's rule that queries do not
+// overlap inserts
+// (include/Streaming_Kmer_Hash_Table.hpp:2264-2266, capi/kache_capi.h:16-21); a resize an upsert run triggers happens
+// inside its call, after the queries before it finished. A run is admitted only while its staging fits the byte budget
+// (device memory for the merged batch), so a burst of requests waits rather than exhausting HBM.
+#include "engine.cuh"
+#include "kache_b200.h"
+
+#include <chrono>
+#include <condition_variable>
+#include <deque>
+#include <mutex>
+#include <thread>
+#include <unordered_map>
+#include <vector>
+
+namespace
+{
+
+using clock_type = std::chrono::steady_clock;
+
+struct Request
+{
+    uint64_t ticket;
+    uint32_t kind;                  // KACHE_B200_REQ_*
+    std::vector<const char*> seqs;  // The caller's sequences: they stay the caller's and must outlive the request.
+    std::vector<size_t> lens;
+    uint32_t op;
+    uint64_t x, init;
+    void* out0;                     // lookup: found; count: counts
+    void* out1;                     // lookup: values (or null)
+    void* out2;                     // lookup: fwd (or null)
+    uint64_t positions = 0, bytes = 0, result = 0;
+    int status = KACHE_OK;
+    bool done = false;
+    clock_type::time_point t_submit, t_done;
+};
+
+}
+
+struct kache_server
+{
+    kache_table* t;
+    uint32_t user;
+    uint64_t budget;                // Most staging bytes of one merged run.
+    // Most k-mer positions of one merged run (unless its first request alone has more): enough to keep every SM
+    // busy, few enough that a run's staging buffers stay reused and a request waits behind one run at most this big.
+    static constexpr uint64_t run_positions = uint64_t(1) << 24;
+    std::mutex mu;
+    std::condition_variable cv, done_cv;
+    std::deque<Request*> queue;
+    std::unordered_map<uint64_t, Request*> all;
+    uint64_t next_ticket = 1;
+    bool stop = false;
+    std::thread worker;
+    // Merged outputs, reused across runs, in page-locked memory (the table copies into it directly).
+    kache_b200::Pinned_Buf found, fwd, values, counts;
+    uint64_t runs = 0, merged = 0;
+
+    void loop();
+    void run(std::vector<Request*>& g);
+};
+
+namespace
+{
+
+// Device bytes a request's staging takes: bases, offsets, segment list and per-position outputs.
+uint64_t request_bytes(const Request& r, const uint32_t k, const uint32_t vb)
+{
+    uint64_t bases = 0, pos = 0;
+    for(const size_t len : r.lens)
+        bases += len, pos += len >= k ? len - k + 1 : 0;
+    const uint64_t per_pos = r.kind == KACHE_B200_REQ_LOOKUP ? 2 + vb : 1;
+    return bases + 24 * r.lens.size() + pos * per_pos;
+}
+
+bool compatible(const Request& a, const Request& b)
+{
+    if(a.kind != b.kind)
+        return false;
+    if(a.kind == KACHE_B200_REQ_UPSERT)
+        return a.op == b.op && a.x == b.x && a.init == b.init;
+    if(a.kind == KACHE_B200_REQ_LOOKUP)
+        return (a.out1 == nullptr) == (b.out1 == nullptr) && (a.out2 == nullptr) == (b.out2 == nullptr);
+    return true;
+}
+
+}
+
+void kache_server::loop()
+{
+    for(;;)
+    {
+        std::vector<Request*> g;
+        {
+            std::unique_lock<std::mutex> lk(mu);
+            cv.wait(lk, [&](){ return stop || !queue.empty(); });
+            if(queue.empty())
+                return;
+            // The run: the head, then every waiting request that can merge with it, in arrival order, within budget;
+            // the others keep their order in the queue.
+            uint64_t bytes = 0, pos = 0;
+            std::deque<Request*> rest;
+            for(Request* r : queue)
+                if(g.empty() || (compatible(*r, *g.front()) && bytes + r->bytes <= budget && pos + r->positions <= run_positions))
+                    bytes += r->bytes, pos += r->positions, g.push_back(r);
+                else
+                    rest.push_back(r);
+            queue.swap(rest);
+        }
+        run(g);
+        {
+            std::lock_guard<std::mutex> lk(mu);
+            const auto now = clock_type::now();
+            for(Request* r : g)
+                r->done = true, r->t_done = now;
+            runs++, merged += g.size();
+        }
+        done_cv.notify_all();
+    }
+}
+
+void kache_server::run(std::vector<Request*>& g)
+{
+    std::vector<const char*> seqs;
+    std::vector<size_t> lens;
+    std::vector<size_t> first(g.size() + 1, 0);     // Each request's first sequence in the merged batch.
+    std::vector<uint64_t> pos_first(g.size() + 1, 0);
+    for(size_t i = 0; i < g.size(); ++i)
+    {
+        seqs.insert(seqs.end(), g[i]->seqs.begin(), g[i]->seqs.end());
+        lens.insert(lens.end(), g[i]->lens.begin(), g[i]->lens.end());
+        first[i + 1] = seqs.size();
+        pos_first[i + 1] = pos_first[i] + g[i]->positions;
+    }
+    const size_t n = seqs.size();
+    const Request& h = *g.front();
+    const size_t vb = t->value_bytes;
+    try
+    {
+        if(h.kind == KACHE_B200_REQ_UPSERT)
+        {
+            counts.ensure((n + 1) * 8);
+            const uint64_t* c = counts.as<uint64_t>();
+            t->upsert_split(user, seqs.data(), lens.data(), n, h.op, h.x, h.init, counts.as<uint64_t>());
+            for(size_t i = 0; i < g.size(); ++i)
+            {
+                uint64_t s = 0;
+                for(size_t q = first[i]; q < first[i + 1]; ++q)
+                    s += c[q];
+                g[i]->result = s;
+            }
+        }
+        else if(h.kind == KACHE_B200_REQ_LOOKUP)
+        {
+            const uint64_t P = pos_first.back();
+            found.ensure(P + 16), fwd.ensure(h.out2 ? P + 16 : 16), values.ensure(h.out1 && vb ? P * vb + 16 : 16);
+            const uint8_t* f = found.as<uint8_t>();
+            const uint8_t* vals = values.as<uint8_t>();
+            t->lookup(seqs.data(), lens.data(), n, found.as<uint8_t>(), h.out1 && vb ? values.p : nullptr, h.out2 ? fwd.as<uint8_t>() : nullptr);
+            for(size_t i = 0; i < g.size(); ++i)
+            {
+                const uint64_t a = pos_first[i], m = g[i]->positions;
+                std::memcpy(g[i]->out0, f + a, m);
+                if(g[i]->out1 && vb)
+                    std::memcpy(g[i]->out1, vals + a * vb, m * vb);
+                if(g[i]->out2)
+                    std::memcpy(g[i]->out2, fwd.as<uint8_t>() + a, m);
+                uint64_t hits = 0;
+                for(uint64_t j = 0; j < m; ++j)
+                    hits += f[a + j] == 1;
+                g[i]->result = hits;
+            }
+        }
+        else
+        {
+            counts.ensure((n + 1) * 8);
+            const uint64_t* c = counts.as<uint64_t>();
+            t->seq_reduce(seqs.data(), lens.data(), n, 0, 0, 0, counts.as<uint64_t>());
+            for(size_t i = 0; i < g.size(); ++i)
+            {
+                uint64_t s = 0;
+                for(size_t q = first[i]; q < first[i + 1]; ++q)
+                    s += c[q];
+                std::memcpy(g[i]->out0, c + first[i], (first[i + 1] - first[i]) * sizeof(uint64_t));
+                g[i]->result = s;
+            }
+        }
+    }
+    catch(const std::bad_alloc&)
+    {
+        for(Request* r : g)
+            r->status = KACHE_ENOMEM;
+    }
+    catch(...)
+    {
+        for(Request* r : g)
+            r->status = KACHE_EINTERNAL;
+    }
+}
+
+extern "C" int kache_b200_server_new(kache_table* const t, const uint64_t budget_bytes, kache_server** const out) noexcept
+{
+    if(t == nullptr || out == nullptr)
+        return KACHE_EINVAL;
+    *out = nullptr;
+    try
+    {
+        uint32_t user = 0;
+        {
+            std::lock_guard<std::mutex> g(t->reg);
+            if(t->user_c.load() >= KACHE_MAX_USERS)
+                return KACHE_EUSERS;
+            user = t->user_c++;
+        }
+        auto* s = new kache_server;
+        s->t = t, s->user = user;
+        size_t free_b = 0, total_b = 0;
+        if(cudaMemGetInfo(&free_b, &total_b) != cudaSuccess)
+            free_b = size_t(1) << 30;
+        // The budget: as asked, but at most half the device memory free now.
+        s->budget = std::max<uint64_t>(1, std::min<uint64_t>(budget_bytes ? budget_bytes : ~0ull, free_b / 2));
+        // The merged outputs of a full-size run, page-locked once here rather than while requests wait.
+        const uint64_t P = kache_server::run_positions;
+        s->found.ensure(P + 16), s->values.ensure(P * std::max<uint32_t>(1, t->value_bytes) + 16);
+        s->counts.ensure((P / 16) * 8);
+        s->worker = std::thread([s](){ s->loop(); });
+        *out = s;
+        return KACHE_OK;
+    }
+    catch(const std::bad_alloc&)
+    {
+        return KACHE_ENOMEM;
+    }
+    catch(...)
+    {
+        return KACHE_EINTERNAL;
+    }
+}
+
+extern "C" void kache_b200_server_free(kache_server* const s) noexcept
+{
+    if(s == nullptr)
+        return;
+    {
+        std::lock_guard<std::mutex> lk(s->mu);
+        s->stop = true;
+    }
+    s->cv.notify_all();
+    if(s->worker.joinable())
+        s->worker.join();
+    for(auto& kv : s->all)
+        delete kv.second;
+    delete s;
+}
+
+extern "C" int kache_b200_server_submit(kache_server* const s, const uint32_t kind, const char* const* const seqs, const size_t* const lens, const size_t n,
+                                        const uint32_t op, const uint64_t x, const uint64_t init, void* const out0, void* const out1, void* const out2,
+                                        uint64_t* const ticket) noexcept
+{
+    if(s == nullptr || ticket == nullptr || kind > KACHE_B200_REQ_COUNT || (n > 0 && (seqs == nullptr || lens == nullptr)))
+        return KACHE_EINVAL;
+    if(kind != KACHE_B200_REQ_UPSERT && n > 0 && out0 == nullptr)
+        return KACHE_EINVAL;
+    if(kind == KACHE_B200_REQ_UPSERT && op != KACHE_B200_ADD_WRAP && op > KACHE_MAX)
+        return KACHE_EINVAL;
+    try
+    {
+        auto* r = new Request;
+        r->kind = kind, r->op = op, r->x = x, r->init = init, r->out0 = out0, r->out1 = out1, r->out2 = out2;
+        r->seqs.assign(seqs, seqs + n), r->lens.assign(lens, lens + n);
+        const uint32_t k = s->t->kmer_k;
+        for(const size_t len : r->lens)
+            r->positions += len >= k ? len - k + 1 : 0;
+        r->bytes = request_bytes(*r, k, s->t->value_bytes);
+        r->t_submit = clock_type::now();
+        {
+            std::lock_guard<std::mutex> lk(s->mu);
+            r->ticket = s->next_ticket++;
+            s->all[r->ticket] = r;
+            s->queue.push_back(r);
+        }
+        s->cv.notify_one();
+        *ticket = r->ticket;
+        return KACHE_OK;
+    }
+    catch(const std::bad_alloc&)
+    {
+        return KACHE_ENOMEM;
+    }
+}
+
+extern "C" int kache_b200_server_wait(kache_server* const s, const uint64_t ticket, uint64_t* const result, double* const latency_ms) noexcept
+{
+    if(s == nullptr)
+        return KACHE_EINVAL;
+    std::unique_lock<std::mutex> lk(s->mu);
+    const auto it = s->all.find(ticket);
+    if(it == s->all.end())
+        return KACHE_EINVAL;
+    Request* r = it->second;
+    s->done_cv.wait(lk, [&](){ return r->done; });
+    if(result)
+        *result = r->result;
+    if(latency_ms)
+        *latency_ms = std::chrono::duration<double, std::milli>(r->t_done - r->t_submit).count();
+    const int status = r->status;
+    s->all.erase(it);
+    delete r;
+    return status;
+}
+
+extern "C" int kache_b200_server_stats(kache_server* const s, uint64_t* const runs, uint64_t* const requests) noexcept
+{
+    if(s == nullptr)
+        return KACHE_EINVAL;
+    std::lock_guard<std::mutex> lk(s->mu);
+    if(runs)
+        *runs = s->runs;
+    if(requests)
+        *requests = s->merged;
+    return KACHE_OK;
+}

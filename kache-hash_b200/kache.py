@@ -91,6 +91,11 @@ def lib():
             "kache_b200_profile": (ctypes.c_int, [_vp, ctypes.c_int]),
             "kache_b200_profile_read": (ctypes.c_int, [_vp, ctypes.c_uint32, ctypes.POINTER(ctypes.c_double), _u64p]),
             "kache_b200_kernel_launches": (ctypes.c_uint64, []),
+            "kache_b200_server_new": (ctypes.c_int, [_vp, ctypes.c_uint64, ctypes.POINTER(_vp)]),
+            "kache_b200_server_free": (None, [_vp]),
+            "kache_b200_server_submit": (ctypes.c_int, [_vp, ctypes.c_uint32, _vp, _vp, ctypes.c_size_t, ctypes.c_uint32, ctypes.c_uint64, ctypes.c_uint64, _vp, _vp, _vp, _u64p]),
+            "kache_b200_server_wait": (ctypes.c_int, [_vp, ctypes.c_uint64, _u64p, ctypes.POINTER(ctypes.c_double)]),
+            "kache_b200_server_stats": (ctypes.c_int, [_vp, _u64p, _u64p]),
             "kache_b200_memory_roof": (ctypes.c_int, [ctypes.c_uint64, ctypes.c_uint32, ctypes.c_uint64, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)]),
         }
         for name, (res, args) in sig.items():
@@ -398,3 +403,45 @@ def memory_roof(nbytes, kind, accesses=1 << 27):
     ms, rate = ctypes.c_double(), ctypes.c_double()
     _check(lib().kache_b200_memory_roof(nbytes, kind, accesses, ctypes.byref(ms), ctypes.byref(rate)), "kache_b200_memory_roof")
     return ms.value, rate.value
+
+
+REQ_UPSERT, REQ_LOOKUP, REQ_COUNT = 0, 1, 2
+
+
+class Server:
+    """The request server over a table (kache_b200_server_*): submit from any thread, wait for each ticket."""
+
+    def __init__(self, table, budget_bytes=0):
+        h = _vp()
+        _check(lib().kache_b200_server_new(table.h, budget_bytes, ctypes.byref(h)), "kache_b200_server_new")
+        self.h, self.table, self.keep = h, table, {}
+
+    def submit(self, kind, b, op=0, x=0, init=0, out0=None, out1=None, out2=None):
+        t = ctypes.c_uint64()
+        _check(lib().kache_b200_server_submit(self.h, kind, *b.args(), op, x, init, _p(out0), _p(out1), _p(out2), ctypes.byref(t)),
+               "kache_b200_server_submit")
+        self.keep[t.value] = (b, out0, out1, out2)    # The request's buffers live until it completes.
+        return t.value
+
+    def wait(self, ticket):
+        r, ms = ctypes.c_uint64(), ctypes.c_double()
+        code = lib().kache_b200_server_wait(self.h, ticket, ctypes.byref(r), ctypes.byref(ms))
+        self.keep.pop(ticket, None)
+        _check(code, "kache_b200_server_wait")
+        return r.value, ms.value
+
+    def stats(self):
+        a, b = ctypes.c_uint64(), ctypes.c_uint64()
+        _check(lib().kache_b200_server_stats(self.h, ctypes.byref(a), ctypes.byref(b)), "kache_b200_server_stats")
+        return a.value, b.value
+
+    def close(self):
+        if self.h:
+            lib().kache_b200_server_free(self.h)
+            self.h = _vp()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

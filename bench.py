@@ -345,7 +345,7 @@ def run_b200(args):
     # The random-access roofline: a launch's streamed bytes at the copy peak plus its random slot-sector reads and
     # updates at the device's measured random-sector rates (kache_b200_memory_roof over a 1 GiB array, larger than the
     # table); the checksum sectors (the 32*rho term) are left out, as the checksum array (25 MB) stays in L2.
-    roof = random_roofs(kache) if rank == 0 else None
+    roof = random_roofs(kache) if rank == 0 and not args.only_dev else None
     if roof and "error" not in roof:
         streamed = {"upsert": b_in_up * P_up, "lookup": (b_in_find + 9) * P_find}
         reads = {"upsert": P_up * (1 - inserted / P_up), "lookup": P_find * hit}

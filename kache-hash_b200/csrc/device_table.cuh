@@ -152,10 +152,20 @@ struct Op_Fn
     {
         if(op == OP_KEEP)
             return;
+        constexpr V mx = static_cast<V>(~V(0));
         if constexpr(sizeof(V) == 8)
         {
             switch(op)
             {
+            case OP_ADD:
+                // Saturating add as an atomic add, then the saturated value wherever an add carried past the maximum:
+                // every add that overflows sees it (old > max - x) and stores the maximum after its own add, and an
+                // add landing on a value an overflow left small either overflows in turn or is overwritten by that
+                // fix-up, so the word ends at min(max, v + sum x) as the serial order would leave it. Nothing reads
+                // values while inserts run.
+                if(atomicAdd(w, static_cast<unsigned long long>(x)) > static_cast<unsigned long long>(mx - x))
+                    atomicExch(w, static_cast<unsigned long long>(mx));
+                return;
             case OP_ASSIGN: atomicExch(w, static_cast<unsigned long long>(x)); return;
             case OP_OR: atomicOr(w, static_cast<unsigned long long>(x)); return;
             case OP_MIN: atomicMin(w, static_cast<unsigned long long>(x)); return;
@@ -169,6 +179,10 @@ struct Op_Fn
             unsigned int* p = reinterpret_cast<unsigned int*>(w);
             switch(op)
             {
+            case OP_ADD:    // As above, on the value's 32-bit word (values of 1 or 2 bytes saturate below its top).
+                if(atomicAdd(p, static_cast<unsigned int>(x)) > static_cast<unsigned int>(mx - x))
+                    atomicExch(p, static_cast<unsigned int>(mx));
+                return;
             case OP_ASSIGN: atomicExch(p, static_cast<unsigned int>(x)); return;
             case OP_OR: atomicOr(p, static_cast<unsigned int>(x)); return;
             case OP_MIN: atomicMin(p, static_cast<unsigned int>(x)); return;

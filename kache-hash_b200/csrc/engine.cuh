@@ -372,6 +372,7 @@ class Engine final : public kache_table
     static constexpr int out_depth = 4;     // D2H pieces in flight ahead of the copy-out.
     cudaEvent_t ev_out_[out_depth] = {};
     Dev_Buf dbatch_, dout_, dretry_a_, dretry_b_, dscan_, dtmp_;
+    Dev_Buf dhost_;     // A page-locked host batch's bases and offsets, copied as they lie.
 
     // Profiling.
     bool prof_ = false;
@@ -624,8 +625,28 @@ class Engine final : public kache_table
             if(i + 1 < n && seqs[i] + lens[i] != seqs[i + 1])
                 contiguous = false;
         }
-        // Sequences laid end to end in page-locked memory are copied to the device as they lie, with no gather.
+        // Sequences laid end to end in page-locked memory are copied to the device as they lie, with no gather, and
+        // listed in segments there (stage_dev): the host only writes the offsets.
         const bool direct = n > 0 && bytes > 0 && contiguous && pinned(seqs[0]) && pinned(seqs[0] + bytes - 1);
+        if(direct)
+        {
+            pin_.ensure((n + 1) * 8);
+            uint64_t* off = pin_.as<uint64_t>();
+            const char* base = seqs[0];
+            parallel_for(n, 1 << 16, [&](const size_t s, const size_t e)
+            {
+                for(size_t i = s; i < e; ++i)
+                    off[i] = static_cast<uint64_t>(seqs[i] - base);
+            });
+            off[n] = bytes;
+            const size_t o_off = (bytes + 64 + 15) / 16 * 16;
+            dhost_.ensure(o_off + (n + 1) * 8);
+            char* d = dhost_.as<char>();
+            check(cudaMemcpyAsync(d, base, bytes, cudaMemcpyHostToDevice, stream_), "H2D batch");
+            check(cudaMemsetAsync(d + bytes, 0, 64, stream_), "memset");
+            check(cudaMemcpyAsync(d + o_off, off, (n + 1) * 8, cudaMemcpyHostToDevice, stream_), "H2D offsets");
+            return stage_dev(reinterpret_cast<const uint8_t*>(d), reinterpret_cast<const uint64_t*>(d + o_off), n, lanes);
+        }
         const uint32_t seg_len = seg_len_for(lanes, max_pos, all_pos);
         uint64_t nsegs = 0;
         for(size_t i = 0; i < n; ++i)
@@ -635,7 +656,7 @@ class Engine final : public kache_table
         }
         const size_t o_off = 0, o_pos = o_off + (n + 1) * 8, o_seg = o_pos + (n + 1) * 8, o_bases = o_seg + nsegs * 8;
         const size_t total = o_bases + bytes + 64;
-        pin_.ensure(direct ? o_bases + 64 : total);
+        pin_.ensure(total);
         auto* off = pin_.as<uint64_t>(o_off);
         auto* pos_off = pin_.as<uint64_t>(o_pos);
         auto* segs = pin_.as<uint64_t>(o_seg);
@@ -671,10 +692,8 @@ class Engine final : public kache_table
         dbatch_.ensure(total);
         char* d = dbatch_.as<char>();
         check(cudaMemcpyAsync(d, pin_.p, o_bases, cudaMemcpyHostToDevice, stream_), "H2D batch");
-        if(direct)
-            check(cudaMemcpyAsync(d + o_bases, seqs[0], bytes, cudaMemcpyHostToDevice, stream_), "H2D batch");
         constexpr uint64_t piece = uint64_t(32) << 20;
-        for(size_t i0 = direct ? n : 0; i0 < n; )
+        for(size_t i0 = 0; i0 < n; )
         {
             size_t i1 = i0;
             while(i1 < n && off[i1] - off[i0] < piece)
@@ -982,6 +1001,24 @@ class Engine final : public kache_table
         return a.type == cudaMemoryTypeHost;
     }
 
+    // The device address of `bytes` of page-locked host memory at p (one allocation, mapped into the device's address
+    // space, as cudaHostAlloc'd memory is on 64-bit systems), or null.
+    static void* mapped(void* p, const size_t bytes)
+    {
+        if(p == nullptr || bytes == 0)
+            return nullptr;
+        cudaPointerAttributes a{}, z{};
+        if(cudaPointerGetAttributes(&a, p) != cudaSuccess || cudaPointerGetAttributes(&z, static_cast<char*>(p) + bytes - 1) != cudaSuccess)
+        {
+            (void)cudaGetLastError();
+            return nullptr;
+        }
+        if(a.type != cudaMemoryTypeHost || z.type != cudaMemoryTypeHost || a.devicePointer == nullptr || z.devicePointer == nullptr ||
+           static_cast<char*>(z.devicePointer) - static_cast<char*>(a.devicePointer) != static_cast<ptrdiff_t>(bytes - 1))
+            return nullptr;
+        return a.devicePointer;
+    }
+
     // Copies device output to a host buffer. Into page-locked memory, one copy. Into pageable memory, through pinned
     // pieces: up to `out_depth` D2H copies run ahead while the host pool copies finished pieces out.
     void d2h(void* dst, const void* src, const size_t bytes)
@@ -1130,6 +1167,20 @@ public:
         const auto bi = stage_host(seqs, lens, n, false);
         const uint64_t P = bi.total_pos;
         const size_t vb = (!set_ && values) ? sizeof(VT) : 0;
+        // Outputs in page-locked memory that the device can address: the kernel writes them there itself, its
+        // stores crossing PCIe while it computes, with no copy after it.
+        if(P > 0)
+        {
+            void* m_found = mapped(found, P);
+            void* m_val = vb ? mapped(values, P * vb) : nullptr;
+            void* m_fwd = fwd ? mapped(fwd, P) : nullptr;
+            if(m_found && (!vb || m_val) && (!fwd || m_fwd))
+            {
+                run_lookup(bi, static_cast<uint8_t*>(m_found), static_cast<VT*>(m_val), static_cast<uint8_t*>(m_fwd));
+                sync();
+                return;
+            }
+        }
         const size_t a_found = (P + 15) / 16 * 16, a_val = (P * vb + 15) / 16 * 16;
         dout_.ensure(a_found + a_val + P + 64);
         uint8_t* d_found = dout_.as<uint8_t>();

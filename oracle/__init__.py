@@ -39,6 +39,7 @@ class Oracle:
             "orc_minimizer_hash": (_u64, [_u64, ctypes.c_int, ctypes.c_int]),
             "orc_describe": (_u64, [_vp, _u64, ctypes.c_int, ctypes.c_int, _vp, _vp, _vp, _vp, _vp]),
             "orc_cap_for": (_u64, [_u64, ctypes.c_double, ctypes.c_int]),
+            "orc_replay_capacity": (None, [_u64, ctypes.c_double, ctypes.c_int, _vp, _u64, _vp]),
             "orc_fits": (ctypes.c_int, [_u64, ctypes.c_double, ctypes.c_int]),
             "orc_new": (_vp, [ctypes.c_int, ctypes.c_int, _u64, ctypes.c_double, ctypes.c_int]),
             "orc_free": (None, [_vp]),
@@ -290,3 +291,11 @@ class RefTable:
         c = self.L.ref_dump(self.h, keys.ctypes.data, vals.ctypes.data)
         o = np.argsort(keys[:c], kind="stable")
         return keys[:c][o], (vals[:c][o] if self.vb else None)
+
+
+def replay_capacity(n, lf, pow2, inserted):
+    """The capacity after each call of one user whose calls inserted `inserted` keys (orc_replay_capacity)."""
+    ins = np.ascontiguousarray(inserted, dtype=np.uint64)
+    caps = np.zeros(max(len(ins), 1), np.uint64)
+    oracle().L.orc_replay_capacity(n, lf, 1 if pow2 else 0, ins.ctypes.data, len(ins), caps.ctypes.data)
+    return caps[:len(ins)]

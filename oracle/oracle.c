@@ -490,3 +490,21 @@ void orc_histogram(const orc_table* t, const uint64_t max, uint64_t* h)
         if(t->key[i] != EMPTY && t->val[i] >= 1 && t->val[i] <= max)
             h[t->val[i]]++;
 }
+
+/* The capacity (in slots) after each of a single user's calls that inserted ins[0..calls) keys, into a table sized
+ * for max_sz keys: the schedule of account() alone, for checking capacities at sizes the exact dictionary would not
+ * hold. */
+void orc_replay_capacity(const uint64_t max_sz, const double lf, const int pow2, const uint64_t* ins, const uint64_t calls, uint64_t* caps)
+{
+    orc_table t;
+    memset(&t, 0, sizeof(t));
+    t.lf = lf;
+    t.cap = orc_cap_for(max_sz, lf, pow2);
+    t.resize_th = (uint64_t)((double)(t.cap * B) * lf);
+    t.step = step_for(t.resize_th);
+    for(uint64_t i = 0; i < calls; ++i)
+    {
+        account(&t, 0, ins[i]);
+        caps[i] = t.cap * B;
+    }
+}

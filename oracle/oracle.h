@@ -39,6 +39,7 @@ uint64_t orc_minimizer_hash(uint64_t key, int k, int l);
 uint64_t orc_describe(const char* s, uint64_t len, int k, int l, uint64_t* key, uint64_t* h, uint8_t* cs, uint8_t* fwd, uint8_t* valid);
 
 uint64_t orc_cap_for(uint64_t max_sz, double lf, int pow2);
+void orc_replay_capacity(uint64_t max_sz, double lf, int pow2, const uint64_t* ins, uint64_t calls, uint64_t* caps);
 int orc_fits(uint64_t max_sz, double lf, int pow2);
 
 typedef struct orc_table orc_table;

@@ -117,3 +117,20 @@ def test_oracle_against_live_reference(k, vb, n, pow2, op):
         for b in (reads.slice(0, 100), reads.slice(100, 300)):
             assert R.update(b, 16, 3) == O.update(b, 16, 3)
         assert np.array_equal(R.dump()[1], O.dump()[1])
+
+
+@pytest.mark.skipif(oracle.ref() is None, reason="the reference was not built on this machine")
+@pytest.mark.parametrize("k,n,lf,pow2", [(32, 1000, 0.8, False), (31, 300, 0.9, True)])
+def test_capacity_replay_against_live_reference(k, n, lf, pow2):
+    """The schedule replay used at full sizes (oracle.replay_capacity) gives the reference's capacity after each call
+    from the call's inserted count alone."""
+    g = synth.genome(300_000, seed=211)
+    reads = Batch(*synth.reads_fixed(g, 6000, 150, seed=212))
+    R = oracle.RefTable(k, 0, n, lf, pow2, workers=2)
+    u = R.register()
+    ins, caps = [], []
+    for i in range(0, reads.n, 250):
+        ins.append(R.upsert(u, reads.slice(i, min(i + 250, reads.n)), 0, 0))
+        caps.append(R.capacity())
+    assert list(oracle.replay_capacity(n, lf, pow2, ins)) == caps
+    assert caps[-1] > caps[0]

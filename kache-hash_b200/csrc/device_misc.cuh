@@ -309,6 +309,77 @@ static __global__ void batch_counts_kernel(const uint64_t* off, const uint64_t n
         atomicOr(too_long, 1u);
 }
 
+// All of a small device batch's staging in one block of 1024 threads: each thread takes a run of sequences, their
+// positions and segments are summed over the block (pos_off, and the segment list at `segs` if it has room for
+// seg_cap entries), and out[0..2] get the positions, the segments and whether a sequence has more segments than a
+// list entry indexes. In place of a counting kernel, two scans, a listing kernel and their copies.
+constexpr uint32_t small_stage_max = 1u << 16;     // Sequences of a batch staged by one block.
+
+static __global__ void __launch_bounds__(1024) stage_small_kernel(const uint64_t* off, const uint64_t n, const int k, const uint32_t seg_len,
+                                                                 uint64_t* pos_off, uint64_t* segs, const uint64_t seg_cap, unsigned long long* out)
+{
+    __shared__ unsigned long long wp[32], ws[32];
+    __shared__ unsigned int long_seq;
+    const uint32_t t = threadIdx.x, lane = t & 31, wid = t >> 5;
+    if(t == 0)
+        long_seq = 0;
+    const uint64_t per = (n + 1023) / 1024, q0 = min(n, uint64_t(t) * per), q1 = min(n, q0 + per);
+    unsigned long long P = 0, S = 0;
+    bool too_long = false;
+    for(uint64_t q = q0; q < q1; ++q)
+    {
+        const uint64_t len = off[q + 1] - off[q];
+        const uint64_t np = len >= uint64_t(k) ? len - k + 1 : 0, ns = (np + seg_len - 1) / seg_len;
+        P += np, S += ns;
+        too_long |= ns > max_seg_index + 1;
+    }
+    // Exclusive prefix sums over the block: within warps by shuffles, then over the warps' totals.
+    unsigned long long ip = P, is = S;
+#pragma unroll
+    for(int o = 1; o < 32; o <<= 1)
+    {
+        const unsigned long long a = __shfl_up_sync(0xFFFFFFFFu, ip, o), b = __shfl_up_sync(0xFFFFFFFFu, is, o);
+        if(lane >= static_cast<uint32_t>(o))
+            ip += a, is += b;
+    }
+    if(lane == 31)
+        wp[wid] = ip, ws[wid] = is;
+    __syncthreads();
+    if(too_long)
+        atomicOr(&long_seq, 1u);
+    if(wid == 0)
+    {
+        unsigned long long a = wp[lane], b = ws[lane];
+#pragma unroll
+        for(int o = 1; o < 32; o <<= 1)
+        {
+            const unsigned long long x = __shfl_up_sync(0xFFFFFFFFu, a, o), y = __shfl_up_sync(0xFFFFFFFFu, b, o);
+            if(lane >= static_cast<uint32_t>(o))
+                a += x, b += y;
+        }
+        wp[lane] = a, ws[lane] = b;
+    }
+    __syncthreads();
+    unsigned long long bp = ip - P + (wid ? wp[wid - 1] : 0), bs = is - S + (wid ? ws[wid - 1] : 0);
+    const unsigned long long total_s = ws[31];
+    for(uint64_t q = q0; q < q1; ++q)
+    {
+        const uint64_t len = off[q + 1] - off[q];
+        const uint64_t np = len >= uint64_t(k) ? len - k + 1 : 0, ns = (np + seg_len - 1) / seg_len;
+        pos_off[q] = bp;
+        if(total_s <= seg_cap && ns <= max_seg_index + 1)
+            for(uint64_t s = 0; s < ns; ++s)
+                segs[bs + s] = (q << 24) | s;
+        bp += np, bs += ns;
+    }
+    __syncthreads();
+    if(t == 1023)
+    {
+        pos_off[n] = wp[31];
+        out[0] = wp[31], out[1] = total_s, out[2] = long_seq;
+    }
+}
+
 static __global__ void batch_segs_kernel(const uint64_t* seg_off, const uint64_t n, uint64_t* segs)
 {
     const uint64_t q = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x;

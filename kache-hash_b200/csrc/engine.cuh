@@ -714,9 +714,56 @@ class Engine final : public kache_table
         return bi;
     }
 
+    // stage_dev for a batch of at most small_stage_max sequences: one block does the counting, the sums and the list.
+    Batch_Info stage_dev_small(const uint8_t* bases, const uint64_t* off, const uint64_t n, const bool lanes)
+    {
+        dtmp_.ensure((n + 1) * 8);
+        uint64_t* pos_off = dtmp_.as<uint64_t>();
+        unsigned long long* out = ctr() + 3;    // Three words: positions, segments, too long.
+        uint64_t* h = pin_ctr_.as<uint64_t>(32);
+        uint32_t seg_len = first_seg_len(lanes, ~0ull);
+        bool sized = false;
+        dbatch_.ensure(8 * n + 8);
+        for(;;)
+        {
+            const uint64_t cap = dbatch_.bytes / 8;
+            launch(K_OTHER, [&](){ stage_small_kernel<<<1, 1024, 0, stream_>>>(off, n, k, seg_len, pos_off, dbatch_.as<uint64_t>(), cap, out); });
+            check(cudaMemcpyAsync(h, out, 24, cudaMemcpyDeviceToHost, stream_), "D2H");
+            sync();
+            if(h[2])
+            {
+                seg_len *= 8;   // A sequence has more segments than a list entry indexes.
+                sized = true;
+                continue;
+            }
+            if(!sized && lanes)
+            {
+                sized = true;
+                const uint32_t want = first_seg_len(lanes, h[0]);
+                if(want != seg_len)
+                {
+                    seg_len = want;
+                    continue;
+                }
+            }
+            if(h[1] > cap)
+            {
+                dbatch_.ensure(h[1] * 8 + 8);   // The list did not fit: list again into a larger one.
+                continue;
+            }
+            break;
+        }
+        Batch_Info bi;
+        bi.b = Dev_Batch{bases, off, dbatch_.as<uint64_t>(), pos_off, n, h[1], seg_len};
+        bi.total_pos = h[0];
+        return bi;
+    }
+
     // Prepares a batch already in device memory: positions and segments computed on the device.
     Batch_Info stage_dev(const uint8_t* bases, const uint64_t* off, const uint64_t n, const bool lanes)
     {
+        if(n > 0 && n <= small_stage_max)
+            return stage_dev_small(bases, off, n, lanes);
         const size_t o_npos = 0, o_nseg = o_npos + (n + 1) * 8, o_pos = o_nseg + (n + 1) * 8, o_sego = o_pos + (n + 1) * 8;
         const size_t head = o_sego + (n + 1) * 8;
         dtmp_.ensure(head);

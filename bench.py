@@ -638,6 +638,7 @@ def run_config4(args):
     torch.cuda.synchronize()
     rz_ms, rz_n = T.profile_read(4)
     up_ms, up_n = T.profile_read(0)
+    ot_ms, ot_n = T.profile_read(5)
     T.profile(False)
     size, cap = T.size(), T.capacity()
     T.close()
@@ -648,7 +649,8 @@ def run_config4(args):
                 {"workload": f"config 4 at scale {args.scale}: {len(g)} bp genome as {bs.n} pieces of 150 bp, calls of 65,536 pieces",
                  "positions": P, "inserted": ins["n"], "keys": size, "capacity": cap},
                 cpu=cpu, extra={"profile_one_step": {"insert_ms": up_ms, "insert_launches": up_n, "rebuild_ms": rz_ms,
-                                                     "rebuild_launches": rz_n}})
+                                                     "rebuild_launches": rz_n, "staging_and_other_ms": ot_ms,
+                                                     "staging_and_other_launches": ot_n}})
 
 
 def run_config5(args):

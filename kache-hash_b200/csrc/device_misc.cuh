@@ -309,14 +309,14 @@ static __global__ void batch_counts_kernel(const uint64_t* off, const uint64_t n
         atomicOr(too_long, 1u);
 }
 
-// All of a small device batch's staging in one block of 1024 threads: each thread takes a run of sequences, their
-// positions and segments are summed over the block (pos_off, and the segment list at `segs` if it has room for
-// seg_cap entries), and out[0..2] get the positions, the segments and whether a sequence has more segments than a
-// list entry indexes. In place of a counting kernel, two scans, a listing kernel and their copies.
-constexpr uint32_t small_stage_max = 1u << 16;     // Sequences of a batch staged by one block.
+// The counting and summing of a small device batch's staging in one block of 1024 threads: each thread takes a run
+// of sequences; pos_off[0..n] and seg_off[0..n] get the exclusive sums of positions and segments, and out[0..2] the
+// positions, the segments and whether a sequence has more segments than a list entry indexes. In place of a counting
+// kernel, two scans and their copies; segs_kernel then lists the segments.
+constexpr uint32_t small_stage_max = 1u << 16;     // Sequences of a batch summed by one block.
 
 static __global__ void __launch_bounds__(1024) stage_small_kernel(const uint64_t* off, const uint64_t n, const int k, const uint32_t seg_len,
-                                                                 uint64_t* pos_off, uint64_t* segs, const uint64_t seg_cap, unsigned long long* out)
+                                                                 uint64_t* pos_off, uint64_t* seg_off, unsigned long long* out)
 {
     __shared__ unsigned long long wp[32], ws[32];
     __shared__ unsigned int long_seq;
@@ -361,32 +361,39 @@ static __global__ void __launch_bounds__(1024) stage_small_kernel(const uint64_t
     }
     __syncthreads();
     unsigned long long bp = ip - P + (wid ? wp[wid - 1] : 0), bs = is - S + (wid ? ws[wid - 1] : 0);
-    const unsigned long long total_s = ws[31];
     for(uint64_t q = q0; q < q1; ++q)
     {
         const uint64_t len = off[q + 1] - off[q];
         const uint64_t np = len >= uint64_t(k) ? len - k + 1 : 0, ns = (np + seg_len - 1) / seg_len;
-        pos_off[q] = bp;
-        if(total_s <= seg_cap && ns <= max_seg_index + 1)
-            for(uint64_t s = 0; s < ns; ++s)
-                segs[bs + s] = (q << 24) | s;
+        pos_off[q] = bp, seg_off[q] = bs;
         bp += np, bs += ns;
     }
-    __syncthreads();
     if(t == 1023)
     {
-        pos_off[n] = wp[31];
-        out[0] = wp[31], out[1] = total_s, out[2] = long_seq;
+        pos_off[n] = wp[31], seg_off[n] = ws[31];
+        out[0] = wp[31], out[1] = ws[31], out[2] = long_seq;
     }
 }
 
-static __global__ void batch_segs_kernel(const uint64_t* seg_off, const uint64_t n, uint64_t* segs)
+// Lists the segments, one thread per segment: its sequence by binary search in seg_off[0..n] (exclusive sums of
+// segments per sequence), so that long sequences' many segments are listed in parallel.
+static __global__ void segs_kernel(const uint64_t* seg_off, const uint64_t n, const uint64_t nsegs, uint64_t* segs)
 {
-    const uint64_t q = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x;
-    if(q >= n)
-        return;
-    for(uint64_t g = seg_off[q], s = 0; g < seg_off[q + 1]; ++g, ++s)
-        segs[g] = (q << 24) | s;
+    const uint64_t stride = uint64_t(gridDim.x) * blockDim.x;
+    for(uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < nsegs; i += stride)
+    {
+        uint64_t lo = 0, hi = n;      // The last q with seg_off[q] <= i.
+        while(hi - lo > 1)
+        {
+            const uint64_t mid = (lo + hi) / 2;
+            if(seg_off[mid] <= i)
+                lo = mid;
+            else
+                hi = mid;
+        }
+        segs[i] = (lo << 24) | (i - seg_off[lo]);
+    }
 }
+
 
 }

@@ -502,7 +502,8 @@ class Engine final : public kache_table
         const uint64_t main_slots = old_cap * B, total = main_slots + ov_slots_;
         dretry_a_.ensure(total / 8 + 8), dretry_b_.ensure(total / 8 + 8);
         check(cudaMemsetAsync(dretry_a_.p, 0, main_slots / 8, stream_), "memset");
-        check(cudaMemsetAsync(dretry_a_.as<char>() + main_slots / 8, 0xFF, ov_slots_ / 8, stream_), "memset");
+        // Every overflow slot is marked for the second phase, unless the overflow table holds no key.
+        check(cudaMemsetAsync(dretry_a_.as<char>() + main_slots / 8, ov_keys ? 0xFF : 0, ov_slots_ / 8, stream_), "memset");
         unsigned int* retried = reinterpret_cast<unsigned int*>(ctr() + 2);
         check(cudaMemsetAsync(retried, 0, 4, stream_), "memset");
         check(cudaMemsetAsync(dretry_b_.p, 0, total / 8 + 8, stream_), "memset");
@@ -714,20 +715,19 @@ class Engine final : public kache_table
         return bi;
     }
 
-    // stage_dev for a batch of at most small_stage_max sequences: one block does the counting, the sums and the list.
+    // stage_dev for a batch of at most small_stage_max sequences: one block counts and sums, one kernel lists.
     Batch_Info stage_dev_small(const uint8_t* bases, const uint64_t* off, const uint64_t n, const bool lanes)
     {
-        dtmp_.ensure((n + 1) * 8);
+        dtmp_.ensure(2 * (n + 1) * 8);
         uint64_t* pos_off = dtmp_.as<uint64_t>();
+        uint64_t* seg_off = pos_off + (n + 1);
         unsigned long long* out = ctr() + 3;    // Three words: positions, segments, too long.
         uint64_t* h = pin_ctr_.as<uint64_t>(32);
         uint32_t seg_len = first_seg_len(lanes, ~0ull);
         bool sized = false;
-        dbatch_.ensure(8 * n + 8);
         for(;;)
         {
-            const uint64_t cap = dbatch_.bytes / 8;
-            launch(K_OTHER, [&](){ stage_small_kernel<<<1, 1024, 0, stream_>>>(off, n, k, seg_len, pos_off, dbatch_.as<uint64_t>(), cap, out); });
+            launch(K_OTHER, [&](){ stage_small_kernel<<<1, 1024, 0, stream_>>>(off, n, k, seg_len, pos_off, seg_off, out); });
             check(cudaMemcpyAsync(h, out, 24, cudaMemcpyDeviceToHost, stream_), "D2H");
             sync();
             if(h[2])
@@ -746,15 +746,14 @@ class Engine final : public kache_table
                     continue;
                 }
             }
-            if(h[1] > cap)
-            {
-                dbatch_.ensure(h[1] * 8 + 8);   // The list did not fit: list again into a larger one.
-                continue;
-            }
             break;
         }
+        const uint64_t nsegs = h[1];
+        dbatch_.ensure(nsegs * 8 + 8);
+        if(nsegs > 0)
+            launch(K_OTHER, [&](){ segs_kernel<<<grid_for((nsegs + 31) / 32, 8), 256, 0, stream_>>>(seg_off, n, nsegs, dbatch_.as<uint64_t>()); });
         Batch_Info bi;
-        bi.b = Dev_Batch{bases, off, dbatch_.as<uint64_t>(), pos_off, n, h[1], seg_len};
+        bi.b = Dev_Batch{bases, off, dbatch_.as<uint64_t>(), pos_off, n, nsegs, seg_len};
         bi.total_pos = h[0];
         return bi;
     }
@@ -815,8 +814,8 @@ class Engine final : public kache_table
         }
         const uint64_t total_pos = h[0], nsegs = h[1];
         dbatch_.ensure(nsegs * 8 + 8);
-        if(n > 0)
-            launch(K_OTHER, [&](){ batch_segs_kernel<<<(n + 255) / 256, 256, 0, stream_>>>(seg_off, n, dbatch_.as<uint64_t>()); });
+        if(nsegs > 0)
+            launch(K_OTHER, [&](){ segs_kernel<<<grid_for((nsegs + 31) / 32, 8), 256, 0, stream_>>>(seg_off, n, nsegs, dbatch_.as<uint64_t>()); });
         Batch_Info bi;
         bi.b = Dev_Batch{bases, off, dbatch_.as<uint64_t>(), pos_off, n, nsegs, seg_len};
         bi.total_pos = total_pos;

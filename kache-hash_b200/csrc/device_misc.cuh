@@ -313,7 +313,7 @@ static __global__ void batch_counts_kernel(const uint64_t* off, const uint64_t n
 // of sequences; pos_off[0..n] and seg_off[0..n] get the exclusive sums of positions and segments, and out[0..2] the
 // positions, the segments and whether a sequence has more segments than a list entry indexes. In place of a counting
 // kernel, two scans and their copies; segs_kernel then lists the segments.
-constexpr uint32_t small_stage_max = 1u << 16;     // Sequences of a batch summed by one block.
+constexpr uint32_t small_stage_max = 4096;  // Sequences of a batch summed by one block (at most 4 per thread).
 
 static __global__ void __launch_bounds__(1024) stage_small_kernel(const uint64_t* off, const uint64_t n, const int k, const uint32_t seg_len,
                                                                  uint64_t* pos_off, uint64_t* seg_off, unsigned long long* out)

@@ -282,7 +282,7 @@ inline bool host_acgt(const char c)
 // Picks the lane kernel's segment length -- positions per lane, which sets how many lanes a batch has and how much of
 // each lane's rolling is warm-up -- per operation (upsert, update, per-sequence reduction) and batch size class (the
 // log2 of its positions), online: the first calls of a class try each candidate, in turn from the built-in choice;
-// later calls take the fastest per position (a moving average of the measured kernel time), and every 16th call
+// later calls take the fastest per position (a moving average of the measured kernel time), and every 64th call
 // retries another candidate so the averages follow the table as it fills.
 class Seg_Tuner
 {
@@ -307,8 +307,8 @@ public:
         for(int c = 1; c < cands; ++c)
             if(s.ns_per_pos[c] < s.ns_per_pos[best])
                 best = c;
-        if(++s.calls % 16 == 0)
-            return (best + 1 + static_cast<int>(s.calls / 16) % (cands - 1)) % cands;
+        if(++s.calls % 64 == 0)
+            return (best + 1 + static_cast<int>(s.calls / 64) % (cands - 1)) % cands;
         return best;
     }
 
@@ -366,6 +366,7 @@ class Engine final : public kache_table
     uint64_t cap_, resize_th_, step_, approx_sz_ = 0, size_ = 0;
     uint64_t pending_[KACHE_MAX_USERS] = {};
     double novelty_ = 0.5;      // Keys inserted per position in the last upsert call.
+    bool novelty_seen_ = false; // Whether an upsert call has measured it.
 
     // Batches.
     Pinned_Buf pin_, pin_ctr_, pin_out_;
@@ -381,6 +382,7 @@ class Engine final : public kache_table
     // The autotuner, and the current call's choice and lane-kernel event pairs.
     Seg_Tuner tuner_;
     int tune_kind_ = -1, tune_cand_ = -1;
+    uint32_t last_seg_len_[3] = {lane_seg_positions, lane_seg_positions, lane_seg_positions};   // Per tuned kind.
     uint64_t tune_pos_ = 0;
     std::vector<std::pair<cudaEvent_t, cudaEvent_t>> tune_ev_;
     size_t tune_used_ = 0;
@@ -579,11 +581,13 @@ class Engine final : public kache_table
     {
         if(!lanes)
             return seg_positions;
-        if(total_pos == ~0ull || tune_kind_ < 0)
+        if(tune_kind_ < 0)
             return builtin_seg_len(total_pos);
+        if(total_pos == ~0ull)
+            return last_seg_len_[tune_kind_];     // Before counting: likely the length this kind's last call used.
         tune_cand_ = tuner_.pick(tune_kind_, total_pos, builtin_seg_len(total_pos));
         tune_pos_ = total_pos;
-        return Seg_Tuner::len[tune_cand_];
+        return last_seg_len_[tune_kind_] = Seg_Tuner::len[tune_cand_];
     }
 
     // Starts a tuned call of `kind` (0 upsert, 1 update, 2 per-sequence reduction); finish_tune() records it.
@@ -922,11 +926,16 @@ class Engine final : public kache_table
             return;
         const uint64_t ov_slots = ov_slots_for(std::max<uint64_t>(1024, target));
         const size_t need = target * (B + 32 + B * slot_bytes) + ov_slots * 32;
-        size_t free_b = 0, total_b = 0;
-        check(cudaMemGetInfo(&free_b, &total_b), "cudaMemGetInfo");
-        const size_t held = size_ == 0 ? cs_.bytes + spill_.bytes + slots_.bytes + ov_.bytes : 0;
-        if(need + (size_t(1) << 30) > free_b + held)
-            return;
+        const bool allocated = size_ == 0 && cs_.bytes >= target * B && spill_.bytes >= target * 32 &&
+                               slots_.bytes >= target * B * slot_bytes && ov_.bytes >= ov_slots * 32;
+        if(!allocated)      // The arrays would be allocated: only if they fit in free device memory.
+        {
+            size_t free_b = 0, total_b = 0;
+            check(cudaMemGetInfo(&free_b, &total_b), "cudaMemGetInfo");
+            const size_t held = size_ == 0 ? cs_.bytes + spill_.bytes + slots_.bytes + ov_.bytes : 0;
+            if(need + (size_t(1) << 30) > free_b + held)
+                return;
+        }
         if(size_ != 0)
         {
             resize(target);
@@ -947,8 +956,10 @@ class Engine final : public kache_table
         uint64_t total_ins = 0;
         // Keys inserted per position: as the previous call measured (1/2 before the first), then as the last chunk
         // measured. The device table is first grown to the capacity the schedule would reach at that rate, so that
-        // a call usually runs as one launch, with no rebuild.
+        // a call usually runs as one launch, with no rebuild. Before any call has measured it, the first chunk is
+        // sized as if every position inserted a key, so that a table fed only new keys is never overfilled.
         double novelty = novelty_;
+        bool assume_all_new = !novelty_seen_;
         grow_ahead(predicted_cap(user, static_cast<uint64_t>(novelty * static_cast<double>(bi.total_pos))));
         Call_Acct acct(Sched{approx_sz_, cap_, resize_th_, step_, lf_}, pending_[user]);
         const size_t bits = bi.total_pos / 8 + 8;
@@ -962,14 +973,18 @@ class Engine final : public kache_table
                 check(cudaMemsetAsync(dretry_a_.p, 0, dretry_a_.bytes, stream_), "memset");
                 dretry_dirty_ = false;
             }
-            // A chunk may take the device table to 95 % of its slots, at a quarter above the expected rate; the
-            // schedule then resizes it, as the reference would.
+            // A chunk may take the device table to 95 % of its slots, at a quarter above the expected rate (and at
+            // least a quarter of the positions); the schedule then resizes it, as the reference would.
             const double slots = static_cast<double>(T_.cap * B);
             const double room = std::max(0.95 * slots - static_cast<double>(size_), 0.05 * slots);
-            const double want_pos = room / std::max(1.25 * novelty, 1e-3);
+            const double rate = assume_all_new ? 1.0 : std::max(1.25 * novelty, 0.25);
+            const double want_pos = room / rate;
             uint64_t se = sb + std::max<uint64_t>(1, static_cast<uint64_t>(want_pos / pos_per_seg));
-            if(se + (se - sb) / 2 >= nsegs)
-                se = nsegs;     // No small last chunk: it would run with too few lanes to fill the GPU.
+            // No small last chunk (it would run with too few lanes to fill the GPU), if the rest fits at the rate.
+            if(se + (se - sb) / 2 >= nsegs && static_cast<double>(nsegs - sb) * pos_per_seg * rate <= 1.25 * room)
+                se = nsegs;
+            se = std::min(se, nsegs);
+            assume_all_new = false;
 
             check(cudaMemsetAsync(ctr(), 0, 8, stream_), "memset");
             check(cudaMemsetAsync(retried, 0, 4, stream_), "memset");
@@ -1003,7 +1018,7 @@ class Engine final : public kache_table
         }
         pending_[user] = acct.left();
         if(bi.total_pos > 0)
-            novelty_ = std::max(static_cast<double>(total_ins) / static_cast<double>(bi.total_pos), 1e-3);
+            novelty_ = std::max(static_cast<double>(total_ins) / static_cast<double>(bi.total_pos), 1e-3), novelty_seen_ = true;
         return total_ins;
     }
 

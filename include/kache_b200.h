@@ -47,6 +47,32 @@ int kache_b200_update_dev(kache_table* t, const uint8_t* d_bases, const uint64_t
 int kache_b200_lookup_dev(kache_table* t, const uint8_t* d_bases, const uint64_t* d_off, uint64_t n, uint8_t* d_found, void* d_values, uint8_t* d_fwd) KACHE_NOEXCEPT;
 int kache_b200_count_dev(kache_table* t, const uint8_t* d_bases, const uint64_t* d_off, uint64_t n, uint64_t* d_counts) KACHE_NOEXCEPT;
 
+/* Several batches resident in device memory, run as one call (no counterpart in the reference, whose callers make
+ * one call per batch, benchmark/measure.cpp:45-140): their sequences share one segment list and one launch, so many
+ * small batches -- a few hundred reads each -- fill the GPU as one large batch does, while each batch keeps its own
+ * arrays and results. Each sequence is read where its batch holds it; nothing is copied. kind is one of
+ * KACHE_B200_RUN_*; op, x and y are the operation and its operands (upsert: x and init; oriented upsert: x_fwd and
+ * x_rev; update: x). Per batch, `result` is set to the keys it inserted (upserts; a key that two batches of the call
+ * insert is credited to one of them) or the k-mers of it present (update), and to 0 otherwise. Lookups write each
+ * batch's found flags, values and orientations to its out0, out1, out2 (device arrays laid out as kache_lookup's;
+ * out1 and out2 may be NULL); counts write its per-sequence counts to out0 (a device array of n uint64_t). The call
+ * returns synchronised with the table's stream. */
+typedef struct kache_dev_batch {
+    const uint8_t* d_bases;     /* sequence i is d_bases[d_off[i], d_off[i + 1]) */
+    const uint64_t* d_off;      /* n + 1 offsets, in device memory */
+    uint64_t n;
+    void* out0;
+    void* out1;
+    void* out2;
+    uint64_t result;
+} kache_dev_batch;
+#define KACHE_B200_RUN_UPSERT          0u
+#define KACHE_B200_RUN_UPSERT_ORIENTED 1u
+#define KACHE_B200_RUN_UPDATE          2u
+#define KACHE_B200_RUN_LOOKUP          3u
+#define KACHE_B200_RUN_COUNT           4u
+int kache_b200_run_dev_batches(kache_table* t, uint32_t user, uint32_t kind, uint32_t op, uint64_t x, uint64_t y, kache_dev_batch* batches, size_t count) KACHE_NOEXCEPT;
+
 /* kache_b200_count_dev for callers that cannot allocate device memory: no counterpart in the reference.
  *
  * Callers running inside their own memory pool, inside a CUDA graph capture, or in a process that budgets every byte

@@ -56,7 +56,7 @@ __global__ void __launch_bounds__(lane_block) lane_kernel(const Dev_Batch batch,
             p0 = (packed & 0xFFFFFF) * batch.seg_len;
             obase = batch.pos_off[q] + p0;
             npos = static_cast<uint32_t>(min(len - k + 1 - p0, static_cast<uint64_t>(batch.seg_len)));
-            p = batch.bases + b0 + p0;
+            p = batch.seq(q, b0) + p0;
             steps = npos + k - 1;
         }
         const uint32_t wsteps = __reduce_max_sync(0xFFFFFFFFu, steps);

@@ -396,4 +396,70 @@ static __global__ void segs_kernel(const uint64_t* seg_off, const uint64_t n, co
 }
 
 
+
+// Several device batches run as one call. desc holds 8 words per batch -- bases, offsets, sequences, first merged
+// sequence, out0, out1, out2, 0 -- in batch order. For merged sequence q: its batch, its length (the merged offsets are
+// the lengths' sums) and the device address of its first base.
+static __global__ void batches_list_kernel(const uint64_t* desc, const uint64_t count, const uint64_t N, uint64_t* lens,
+                                           uint64_t* addr, uint32_t* batch_of)
+{
+    const uint64_t stride = uint64_t(gridDim.x) * blockDim.x;
+    for(uint64_t q = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; q < N; q += stride)
+    {
+        uint64_t lo = 0, hi = count;    // The last batch whose first merged sequence is at or before q: never empty.
+        while(hi - lo > 1)
+        {
+            const uint64_t mid = (lo + hi) / 2;
+            if(desc[8 * mid + 3] <= q)
+                lo = mid;
+            else
+                hi = mid;
+        }
+        const uint64_t* off = reinterpret_cast<const uint64_t*>(desc[8 * lo + 1]);
+        const uint64_t j = q - desc[8 * lo + 3], a = off[j];
+        lens[q] = off[j + 1] - a;
+        addr[q] = desc[8 * lo] + a;
+        batch_of[q] = static_cast<uint32_t>(lo);
+    }
+}
+
+// The merged position of each batch's first k-mer.
+static __global__ void batches_pos_kernel(const uint64_t* desc, const uint64_t count, const uint64_t* pos_off, uint64_t* pos_base)
+{
+    const uint64_t b = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if(b < count)
+        pos_base[b] = pos_off[desc[8 * b + 3]];
+}
+
+// Per-batch sums of per-sequence counts: each thread adds a run of consecutive sequences, flushing at batch changes.
+static __global__ void batches_sum_kernel(const unsigned long long* per_seq, const uint32_t* batch_of, const uint64_t N,
+                                          unsigned long long* per_batch)
+{
+    const uint64_t threads = uint64_t(gridDim.x) * blockDim.x, t = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    const uint64_t per = (N + threads - 1) / threads, q0 = min(N, t * per), q1 = min(N, q0 + per);
+    unsigned long long acc = 0;
+    uint32_t cur = 0;
+    for(uint64_t q = q0; q < q1; ++q)
+    {
+        const uint32_t b = batch_of[q];
+        if(b != cur && acc)
+            atomicAdd(per_batch + cur, acc), acc = 0;
+        cur = b, acc += per_seq[q];
+    }
+    if(acc)
+        atomicAdd(per_batch + cur, acc);
+}
+
+// Per-sequence results of the merged batch copied to each batch's own array (desc word 4).
+static __global__ void batches_scatter_kernel(const uint64_t* desc, const unsigned long long* per_seq, const uint32_t* batch_of,
+                                              const uint64_t N)
+{
+    const uint64_t stride = uint64_t(gridDim.x) * blockDim.x;
+    for(uint64_t q = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; q < N; q += stride)
+    {
+        const uint64_t b = batch_of[q];
+        reinterpret_cast<unsigned long long*>(desc[8 * b + 4])[q - desc[8 * b + 3]] = per_seq[q];
+    }
+}
+
 }

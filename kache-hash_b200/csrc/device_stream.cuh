@@ -23,6 +23,8 @@ namespace kache_b200
 
 // A batch on the device: sequence q is bases[off[q], off[q+1]); segs lists (q << 24 | s) for the s'th segment, of
 // seg_len positions, of each sequence of at least k bases; pos_off[q] counts the positions of the sequences before q.
+// With seq_addr set (several batches run as one), off only lays the lengths end to end and sequence q's
+// off[q+1] - off[q] bases are read at the device address seq_addr[q], where its own batch holds them.
 struct Dev_Batch
 {
     const uint8_t* bases;
@@ -32,6 +34,12 @@ struct Dev_Batch
     uint64_t n;
     uint64_t nsegs;
     uint32_t seg_len;   // A multiple of 32.
+    const uint64_t* seq_addr = nullptr;
+
+    __device__ __forceinline__ const uint8_t* seq(const uint64_t q, const uint64_t b0) const
+    {
+        return seq_addr ? reinterpret_cast<const uint8_t*>(seq_addr[q]) : bases + b0;
+    }
 };
 
 constexpr int stream_warps = 8;
@@ -116,7 +124,7 @@ __global__ void __launch_bounds__(32 * stream_warps) stream_kernel(const Dev_Bat
         const uint64_t packed = batch.segs[g];
         const uint64_t q = packed >> 24, s = packed & 0xFFFFFF;
         const uint64_t b0 = batch.off[q], len = batch.off[q + 1] - b0;
-        const uint8_t* seq = batch.bases + b0;
+        const uint8_t* seq = batch.seq(q, b0);
         const uint64_t npos = len - k + 1;
         const uint64_t p0 = s * batch.seg_len;
         const uint64_t p1 = min(npos, p0 + batch.seg_len);
@@ -280,6 +288,8 @@ struct Update_Visitor
     unsigned long long* present;
     unsigned long long cnt;
     Bucket_Cache bc;            // Bound by the lane kernel (exact: an update inserts nothing); unbound elsewhere.
+    unsigned long long* per_seq = nullptr;  // If set, k-mers present per sequence are added at per_seq[q] (lane kernel).
+    uint32_t lane_cnt = 0;
     static constexpr int stage_bytes = 0;
 
     __device__ __forceinline__ void lane_cache(uint4* lo, uint4* hi) { bc.lo = lo, bc.hi = hi, bc.b = ~0ull; }
@@ -288,8 +298,12 @@ struct Update_Visitor
     __device__ __forceinline__ void begin(uint8_t*) { cnt = 0; }
     __device__ __forceinline__ void begin_segment(uint64_t) {}
     __device__ __forceinline__ void end_segment(uint64_t, uint32_t) {}
-    __device__ __forceinline__ void lane_begin(uint64_t, bool) {}
-    __device__ __forceinline__ void lane_end(uint64_t, bool) {}
+    __device__ __forceinline__ void lane_begin(uint64_t, bool) { lane_cnt = 0; }
+    __device__ __forceinline__ void lane_end(const uint64_t q, const bool has)
+    {
+        if(per_seq && has && lane_cnt)
+            atomicAdd(per_seq + q, static_cast<unsigned long long>(lane_cnt));
+    }
 
     __device__ __forceinline__ void visit(const Kmer_Desc& d, const uint32_t)
     {
@@ -299,6 +313,7 @@ struct Update_Visitor
         if(v)
             fn.apply(v, d.fwd);
         cnt += __popc(__ballot_sync(0xFFFFFFFFu, v != nullptr));
+        lane_cnt += (v != nullptr);
     }
 
     __device__ __forceinline__ void end(const uint32_t lane) { warp_flush(present, cnt, lane); }
@@ -339,6 +354,31 @@ struct Lookup_Visitor
                 values[o] = v ? value_of<V>(w) : V(0);
         if(fwd)
             fwd[o] = d.valid && d.fwd;
+    }
+};
+
+// Lookups of several batches run as one: each sequence's outputs go to its own batch's arrays, at its positions
+// within that batch.
+template <bool set_, typename V>
+struct Lookup_Batches_Visitor : Lookup_Visitor<set_, V>
+{
+    const uint32_t* batch_of;   // Sequence -> batch.
+    const uint64_t* outs;       // Per batch, 8 words: found, values, fwd at words 4-6 (device addresses, or 0).
+    const uint64_t* pos_base;   // Per batch: the merged position of its first k-mer.
+
+    __device__ __forceinline__ void bind(const uint64_t q)
+    {
+        const uint32_t b = batch_of[q];
+        this->found = reinterpret_cast<uint8_t*>(outs[8 * uint64_t(b) + 4]);
+        this->values = reinterpret_cast<V*>(outs[8 * uint64_t(b) + 5]);
+        this->fwd = reinterpret_cast<uint8_t*>(outs[8 * uint64_t(b) + 6]);
+        this->obase = this->pos_off[q] - pos_base[b];
+    }
+    __device__ __forceinline__ void begin_segment(const uint64_t q) { bind(q); }
+    __device__ __forceinline__ void lane_begin(const uint64_t q, const bool has)
+    {
+        if(has)
+            bind(q);
     }
 };
 

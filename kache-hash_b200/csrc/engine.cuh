@@ -11,7 +11,7 @@
 
 #include "device_misc.cuh"
 #include "device_lanes.cuh"
-#include "kache_capi.h"
+#include "kache_b200.h"
 
 #include <cub/device/device_scan.cuh>
 
@@ -54,6 +54,7 @@ struct kache_table
     virtual uint64_t update_dev(const uint8_t* b, const uint64_t* off, uint64_t n, uint32_t op, uint64_t x) = 0;
     virtual void lookup_dev(const uint8_t* b, const uint64_t* off, uint64_t n, uint8_t* found, void* values, uint8_t* fwd) = 0;
     virtual void count_dev(const uint8_t* b, const uint64_t* off, uint64_t n, uint64_t* counts) = 0;
+    virtual void run_dev_batches(uint32_t user, uint32_t kind, uint32_t op, uint64_t x, uint64_t y, kache_dev_batch* bs, size_t count) = 0;
     virtual bool get(const char* kmer, uint64_t& value) = 0;
     virtual uint64_t size() const = 0;
     virtual uint64_t capacity() const = 0;
@@ -374,6 +375,8 @@ class Engine final : public kache_table
     cudaEvent_t ev_out_[out_depth] = {};
     Dev_Buf dbatch_, dout_, dretry_a_, dretry_b_, dscan_, dtmp_;
     Dev_Buf dhost_;     // A page-locked host batch's bases and offsets, copied as they lie.
+    Dev_Buf dmulti_;    // Several device batches run as one: their descriptors and the merged sequence list.
+    Pinned_Buf pin_multi_;
 
     // Profiling.
     bool prof_ = false;
@@ -1335,6 +1338,107 @@ public:
         run_seq_reduce(bi, 0, 0, 0, reinterpret_cast<unsigned long long*>(counts));
         sync();
         finish_tune();
+    }
+
+    // Several batches in device memory as one call: their sequences are listed as one batch whose lengths lie end to
+    // end and whose sequences are read where they lie (Dev_Batch::seq_addr), so all share one segment list, one
+    // launch and one pass of the resize schedule; results go back to each batch.
+    void run_dev_batches(const uint32_t user, const uint32_t kind, const uint32_t op, const uint64_t x, const uint64_t y,
+                         kache_dev_batch* const bs, const size_t count) override
+    {
+        std::lock_guard<std::mutex> g(work);
+        uint64_t N = 0;
+        for(size_t b = 0; b < count; ++b)
+            bs[b].result = 0, N += bs[b].n;
+        if(N == 0 || ((kind == KACHE_B200_RUN_UPSERT_ORIENTED || kind == KACHE_B200_RUN_UPDATE) && set_))
+            return;
+        // Descriptors, 8 words per batch; the merged list: offsets (N + 1), addresses (N), lengths (N), per-batch
+        // first positions and results (count each), batch of each sequence (N, 32-bit).
+        const size_t o_desc = 0, o_off = o_desc + count * 64, o_addr = o_off + (N + 1) * 8, o_len = o_addr + N * 8;
+        const size_t o_pb = o_len + N * 8, o_res = o_pb + count * 8, o_bof = o_res + count * 8, total = o_bof + N * 4;
+        pin_multi_.ensure(count * 64);
+        auto* hd = pin_multi_.as<uint64_t>();
+        for(size_t b = 0, s = 0; b < count; s += bs[b].n, ++b)
+        {
+            uint64_t* e = hd + 8 * b;
+            e[0] = reinterpret_cast<uint64_t>(bs[b].d_bases), e[1] = reinterpret_cast<uint64_t>(bs[b].d_off);
+            e[2] = bs[b].n, e[3] = s;
+            e[4] = reinterpret_cast<uint64_t>(bs[b].out0), e[5] = reinterpret_cast<uint64_t>(bs[b].out1);
+            e[6] = reinterpret_cast<uint64_t>(bs[b].out2), e[7] = 0;
+        }
+        dmulti_.ensure(total);
+        char* d = dmulti_.as<char>();
+        auto* desc = reinterpret_cast<uint64_t*>(d + o_desc);
+        auto* voff = reinterpret_cast<uint64_t*>(d + o_off);
+        auto* addr = reinterpret_cast<uint64_t*>(d + o_addr);
+        auto* lens = reinterpret_cast<uint64_t*>(d + o_len);
+        auto* pos_base = reinterpret_cast<uint64_t*>(d + o_pb);
+        auto* res = reinterpret_cast<unsigned long long*>(d + o_res);
+        auto* batch_of = reinterpret_cast<uint32_t*>(d + o_bof);
+        check(cudaMemcpyAsync(desc, hd, count * 64, cudaMemcpyHostToDevice, stream_), "H2D descriptors");
+        launch(K_OTHER, [&](){ batches_list_kernel<<<grid_for((N + 31) / 32, 8), 256, 0, stream_>>>(desc, count, N, lens, addr, batch_of); });
+        check(cudaMemsetAsync(voff, 0, 8, stream_), "memset");
+        size_t tmp = 0;
+        check(cub::DeviceScan::InclusiveSum(nullptr, tmp, lens, voff + 1, static_cast<int64_t>(N), stream_), "scan");
+        dscan_.ensure(tmp);
+        check(cub::DeviceScan::InclusiveSum(dscan_.p, tmp, lens, voff + 1, static_cast<int64_t>(N), stream_), "scan");
+
+        const bool lanes = kind != KACHE_B200_RUN_LOOKUP;
+        if(kind == KACHE_B200_RUN_UPSERT || kind == KACHE_B200_RUN_UPSERT_ORIENTED)
+            begin_tune(0);
+        else if(kind == KACHE_B200_RUN_UPDATE)
+            begin_tune(1);
+        else if(kind == KACHE_B200_RUN_COUNT)
+            begin_tune(2);
+        auto bi = stage_dev(nullptr, voff, N, lanes);
+        bi.b.seq_addr = addr;
+        dout_.ensure(N * 8 + 8);
+        auto* per_seq = dout_.as<unsigned long long>();
+        const bool sums = kind != KACHE_B200_RUN_LOOKUP && kind != KACHE_B200_RUN_COUNT;
+        if(kind != KACHE_B200_RUN_LOOKUP)
+            check(cudaMemsetAsync(per_seq, 0, N * 8, stream_), "memset");
+        if(kind == KACHE_B200_RUN_UPSERT)
+            run_upsert(user, bi, op_fn(op, x, y), per_seq);
+        else if(kind == KACHE_B200_RUN_UPSERT_ORIENTED)
+        {
+            if constexpr(!set_)
+                run_upsert(user, bi, Oriented_Op_Fn<VT>{op, static_cast<VT>(x), static_cast<VT>(y)}, per_seq);
+        }
+        else if(kind == KACHE_B200_RUN_UPDATE)
+        {
+            if constexpr(!set_)
+            {
+                check(cudaMemsetAsync(ctr(), 0, 8, stream_), "memset");
+                Update_Visitor<VT, Op_Fn<VT>> vis{T_, op_fn(op, x, 0), ctr(), 0};
+                vis.per_seq = per_seq;
+                stream_launch(K_UPDATE, bi, 0, bi.b.nsegs, vis);
+            }
+        }
+        else if(kind == KACHE_B200_RUN_COUNT)
+        {
+            run_seq_reduce(bi, 0, 0, 0, per_seq);
+            launch(K_OTHER, [&](){ batches_scatter_kernel<<<grid_for((N + 31) / 32, 8), 256, 0, stream_>>>(desc, per_seq, batch_of, N); });
+        }
+        else
+        {
+            launch(K_OTHER, [&](){ batches_pos_kernel<<<static_cast<unsigned>((count + 255) / 256), 256, 0, stream_>>>(desc, count, bi.b.pos_off, pos_base); });
+            Lookup_Batches_Visitor<set_, VT> vis{{T_, bi.b.pos_off, nullptr, nullptr, nullptr, 0}, batch_of, desc, pos_base};
+            stream_launch(K_LOOKUP, bi, 0, bi.b.nsegs, vis, true);
+        }
+        if(sums)
+        {
+            check(cudaMemsetAsync(res, 0, count * 8, stream_), "memset");
+            launch(K_OTHER, [&](){ batches_sum_kernel<<<grid_for((N + 31) / 32 / 64 + 1, 8), 256, 0, stream_>>>(per_seq, batch_of, N, res); });
+            auto* hr = pin_multi_.as<uint64_t>();
+            check(cudaMemcpyAsync(hr, res, count * 8, cudaMemcpyDeviceToHost, stream_), "D2H results");
+            sync();
+            for(size_t b = 0; b < count; ++b)
+                bs[b].result = hr[b];
+        }
+        else
+            sync();
+        if(lanes)
+            finish_tune();
     }
 
     bool get(const char* kmer, uint64_t& value) override

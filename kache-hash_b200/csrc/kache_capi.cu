@@ -375,6 +375,32 @@ int kache_b200_count_dev(kache_table* const t, const uint8_t* const d_bases, con
     return guard([&](){ return t->count_dev(d_bases, d_off, n, d_counts), KACHE_OK; });
 }
 
+int kache_b200_run_dev_batches(kache_table* const t, const uint32_t user, const uint32_t kind, const uint32_t op, const uint64_t x, const uint64_t y, kache_dev_batch* const batches, const size_t count) noexcept
+{
+    if(t == nullptr || kind > KACHE_B200_RUN_COUNT || (count > 0 && batches == nullptr) || count > (size_t(1) << 32))
+        return KACHE_EINVAL;
+    const bool upsert = kind == KACHE_B200_RUN_UPSERT || kind == KACHE_B200_RUN_UPSERT_ORIENTED;
+    if(upsert && !registered(t, user))
+        return KACHE_EINVAL;
+    if(kind == KACHE_B200_RUN_UPSERT && t->value_bytes > 0 && !op_ok(op))
+        return KACHE_EINVAL;
+    if(kind == KACHE_B200_RUN_UPSERT_ORIENTED && (t->value_bytes == 0 || !oriented_op_ok(op, true)))
+        return KACHE_EINVAL;
+    if(kind == KACHE_B200_RUN_UPDATE && (t->value_bytes == 0 || !op_ok(op)))
+        return KACHE_EINVAL;
+    for(size_t b = 0; b < count; ++b)
+    {
+        const kache_dev_batch& e = batches[b];
+        if(e.n > 0 && (e.d_bases == nullptr || e.d_off == nullptr))
+            return KACHE_EINVAL;
+        if(e.n > 0 && (kind == KACHE_B200_RUN_LOOKUP || kind == KACHE_B200_RUN_COUNT) && e.out0 == nullptr)
+            return KACHE_EINVAL;
+        if(kind == KACHE_B200_RUN_LOOKUP && t->value_bytes == 0 && e.out1 != nullptr)
+            return KACHE_EINVAL;
+    }
+    return guard([&](){ return t->run_dev_batches(user, kind, op, x, y, batches, count), KACHE_OK; });
+}
+
 int kache_b200_describe(kache_table* const t, const char* const* const seqs, const size_t* const lens, const size_t n, uint64_t* const key, uint64_t* const h, uint8_t* const cs, uint8_t* const fwd, uint8_t* const valid_out) noexcept
 {
     if(t == nullptr || !valid(seqs, lens, n) || !key || !h || !cs || !fwd || !valid_out)

@@ -44,6 +44,14 @@ class Stats(ctypes.Structure):
                 ("secondary_pct", ctypes.c_double), ("overflow_pct", ctypes.c_double)]
 
 
+class DevBatch(ctypes.Structure):
+    """One batch of kache_b200_run_dev_batches: device pointers to its bases and n + 1 offsets, its output arrays."""
+    _fields_ = [("d_bases", _vp), ("d_off", _vp), ("n", ctypes.c_uint64), ("out0", _vp), ("out1", _vp), ("out2", _vp),
+                ("result", ctypes.c_uint64)]
+
+
+RUN_UPSERT, RUN_UPSERT_ORIENTED, RUN_UPDATE, RUN_LOOKUP, RUN_COUNT = range(5)
+
 KEYS_FN = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, _u64p, ctypes.c_void_p, ctypes.c_size_t)
 
 _lib = None
@@ -85,6 +93,7 @@ def lib():
             "kache_b200_update_dev": (ctypes.c_int, [_vp, _vp, _vp, ctypes.c_uint64, ctypes.c_uint32, ctypes.c_uint64, _u64p]),
             "kache_b200_lookup_dev": (ctypes.c_int, [_vp, _vp, _vp, ctypes.c_uint64, _vp, _vp, _vp]),
             "kache_b200_count_dev": (ctypes.c_int, [_vp, _vp, _vp, ctypes.c_uint64, _vp]),
+            "kache_b200_run_dev_batches": (ctypes.c_int, [_vp, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint64, ctypes.c_uint64, ctypes.POINTER(DevBatch), ctypes.c_size_t]),
             "kache_b200_describe": (ctypes.c_int, [_vp, _vp, _vp, ctypes.c_size_t, _vp, _vp, _vp, _vp, _vp]),
             "kache_b200_histogram": (ctypes.c_int, [_vp, ctypes.c_uint64, _vp]),
             "kache_b200_clear": (ctypes.c_int, [_vp]),
@@ -314,6 +323,16 @@ class Table:
 
     def count_dev(self, d_bases, d_off, n, d_counts):
         _check(lib().kache_b200_count_dev(self.h, d_bases, d_off, n, d_counts), "count_dev")
+
+    def run_dev_batches(self, kind, batches, op=0, x=0, y=0, user=0):
+        """Runs device batches as one call (kache_b200_run_dev_batches). `batches` holds tuples (d_bases, d_off, n[,
+        out0[, out1[, out2]]]) of device pointers; returns each batch's result (keys inserted, k-mers present, or 0)."""
+        arr = (DevBatch * max(1, len(batches)))()
+        for i, b in enumerate(batches):
+            outs = list(b[3:]) + [None] * (6 - len(b))
+            arr[i] = DevBatch(b[0], b[1], b[2], outs[0], outs[1], outs[2], 0)
+        _check(lib().kache_b200_run_dev_batches(self.h, user, kind, op, x, y, arr, len(batches)), "run_dev_batches")
+        return [arr[i].result for i in range(len(batches))]
 
     def clear(self):
         _check(lib().kache_b200_clear(self.h), "kache_b200_clear")

@@ -164,19 +164,32 @@ void kache_server::run(std::vector<Request*>& g)
             const uint8_t* f = found.as<uint8_t>();
             const uint8_t* vals = values.as<uint8_t>();
             t->lookup(seqs.data(), lens.data(), n, found.as<uint8_t>(), h.out1 && vb ? values.p : nullptr, h.out2 ? fwd.as<uint8_t>() : nullptr);
-            for(size_t i = 0; i < g.size(); ++i)
+            // Each request's share of the merged outputs to its own arrays, and its present positions: in parts of the
+            // merged positions on the host pool's threads, a part spanning the requests it overlaps.
+            std::vector<std::atomic<uint64_t>> hits(g.size());
+            const uint8_t* fw = fwd.as<uint8_t>();
+            kache_b200::parallel_for(P, size_t(1) << 20, [&](const size_t s, const size_t e)
             {
-                const uint64_t a = pos_first[i], m = g[i]->positions;
-                std::memcpy(g[i]->out0, f + a, m);
-                if(g[i]->out1 && vb)
-                    std::memcpy(g[i]->out1, vals + a * vb, m * vb);
-                if(g[i]->out2)
-                    std::memcpy(g[i]->out2, fwd.as<uint8_t>() + a, m);
-                uint64_t hits = 0;
-                for(uint64_t j = 0; j < m; ++j)
-                    hits += f[a + j] == 1;
-                g[i]->result = hits;
-            }
+                size_t i = static_cast<size_t>(std::upper_bound(pos_first.begin(), pos_first.end(), s) - pos_first.begin()) - 1;
+                for(uint64_t a = s; a < e; ++i)
+                {
+                    const uint64_t b = std::min<uint64_t>(e, pos_first[i + 1]), m = b - a, at = a - pos_first[i];
+                    if(m == 0)
+                        continue;
+                    std::memcpy(static_cast<uint8_t*>(g[i]->out0) + at, f + a, m);
+                    if(g[i]->out1 && vb)
+                        std::memcpy(static_cast<uint8_t*>(g[i]->out1) + at * vb, vals + a * vb, m * vb);
+                    if(g[i]->out2)
+                        std::memcpy(static_cast<uint8_t*>(g[i]->out2) + at, fw + a, m);
+                    uint64_t c = 0;
+                    for(uint64_t j = a; j < b; ++j)
+                        c += f[j] == 1;
+                    hits[i] += c;
+                    a = b;
+                }
+            });
+            for(size_t i = 0; i < g.size(); ++i)
+                g[i]->result = hits[i].load();
         }
         else
         {

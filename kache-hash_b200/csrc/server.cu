@@ -8,7 +8,9 @@
 // overlap inserts
 // (include/Streaming_Kmer_Hash_Table.hpp:2264-2266, capi/kache_capi.h:16-21); a resize an upsert run triggers happens
 // inside its call, after the queries before it finished. A run is admitted only while its staging fits the byte budget
-// (device memory for the merged batch), so a burst of requests waits rather than exhausting HBM.
+// (device memory for the merged batch), so a burst of requests waits rather than exhausting HBM. Two threads share the
+// work: a stager forms the next run and gathers its reads end to end into one of two page-locked buffers while an
+// executor runs the run before it on the GPU and copies its results out, so the host's copying overlaps the device.
 #include "engine.cuh"
 #include "kache_b200.h"
 
@@ -42,6 +44,19 @@ struct Request
     clock_type::time_point t_submit, t_done;
 };
 
+// A run ready for the GPU: its requests, and their sequences as the table is handed them -- gathered end to end into
+// one of the page-locked staging buffers (slot 0 or 1; the table then copies them to the device as they lie and
+// lists them there), or the callers' own memory (slot -1) for a run too large to stage.
+struct Staged
+{
+    std::vector<Request*> g;
+    int slot = -1;
+    std::vector<const char*> seqs;
+    std::vector<size_t> lens;
+    std::vector<size_t> first;          // Each request's first sequence in the run.
+    std::vector<uint64_t> pos_first;    // Each request's first k-mer position in the run.
+};
+
 }
 
 struct kache_server
@@ -52,19 +67,29 @@ struct kache_server
     // Most k-mer positions of one merged run (unless its first request alone has more): enough to keep every SM
     // busy, few enough that a run's staging buffers stay reused and a request waits behind one run at most this big.
     static constexpr uint64_t run_positions = uint64_t(1) << 24;
+    // Most bases of a run gathered into a staging buffer; larger runs are handed over from the callers' memory.
+    static constexpr uint64_t stage_max = uint64_t(256) << 20;
     std::mutex mu;
-    std::condition_variable cv, done_cv;
+    std::condition_variable cv, done_cv, ready_cv;
     std::deque<Request*> queue;
     std::unordered_map<uint64_t, Request*> all;
     uint64_t next_ticket = 1;
     bool stop = false;
-    std::thread worker;
+    // Two threads: the stager forms runs and gathers their reads into a free staging buffer while the executor runs
+    // the run before on the GPU, so the host's copying overlaps the device's work.
+    std::thread worker, executor;
+    kache_b200::Pinned_Buf stage[2];
+    bool slot_busy[2] = {false, false};
+    std::deque<Staged*> ready;
+    bool staging_done = false;
     // Merged outputs, reused across runs, in page-locked memory (the table copies into it directly).
     kache_b200::Pinned_Buf found, fwd, values, counts;
     uint64_t runs = 0, merged = 0;
 
     void loop();
-    void run(std::vector<Request*>& g);
+    void execute();
+    void gather(Staged& st);
+    void run(Staged& st);
 };
 
 namespace
@@ -102,7 +127,12 @@ void kache_server::loop()
             std::unique_lock<std::mutex> lk(mu);
             cv.wait(lk, [&](){ return stop || !queue.empty(); });
             if(queue.empty())
+            {
+                staging_done = true;
+                lk.unlock();
+                ready_cv.notify_all();
                 return;
+            }
             // The run: the head, then every waiting request that can merge with it, in arrival order, within budget;
             // the others keep their order in the queue.
             uint64_t bytes = 0, pos = 0;
@@ -114,31 +144,104 @@ void kache_server::loop()
                     rest.push_back(r);
             queue.swap(rest);
         }
-        run(g);
+        auto* st = new Staged;
+        st->g = std::move(g);
+        gather(*st);
         {
             std::lock_guard<std::mutex> lk(mu);
-            const auto now = clock_type::now();
-            for(Request* r : g)
-                r->done = true, r->t_done = now;
-            runs++, merged += g.size();
+            ready.push_back(st);
         }
-        done_cv.notify_all();
+        ready_cv.notify_all();
     }
 }
 
-void kache_server::run(std::vector<Request*>& g)
+// The stager's half of a run: lists its sequences and, unless it is too large, gathers them end to end into a free
+// staging buffer (waiting for the executor to release one).
+void kache_server::gather(Staged& st)
 {
-    std::vector<const char*> seqs;
-    std::vector<size_t> lens;
-    std::vector<size_t> first(g.size() + 1, 0);     // Each request's first sequence in the merged batch.
-    std::vector<uint64_t> pos_first(g.size() + 1, 0);
+    const auto& g = st.g;
+    st.first.assign(g.size() + 1, 0), st.pos_first.assign(g.size() + 1, 0);
+    uint64_t bytes = 0;
     for(size_t i = 0; i < g.size(); ++i)
     {
-        seqs.insert(seqs.end(), g[i]->seqs.begin(), g[i]->seqs.end());
-        lens.insert(lens.end(), g[i]->lens.begin(), g[i]->lens.end());
-        first[i + 1] = seqs.size();
-        pos_first[i + 1] = pos_first[i] + g[i]->positions;
+        st.lens.insert(st.lens.end(), g[i]->lens.begin(), g[i]->lens.end());
+        st.first[i + 1] = st.lens.size();
+        st.pos_first[i + 1] = st.pos_first[i] + g[i]->positions;
     }
+    for(const size_t len : st.lens)
+        bytes += len;
+    const size_t n = st.lens.size();
+    if(bytes > stage_max)
+    {
+        for(const Request* r : g)
+            st.seqs.insert(st.seqs.end(), r->seqs.begin(), r->seqs.end());
+        return;
+    }
+    {
+        std::unique_lock<std::mutex> lk(mu);
+        ready_cv.wait(lk, [&](){ return !slot_busy[0] || !slot_busy[1]; });
+        st.slot = slot_busy[0] ? 1 : 0;
+        slot_busy[st.slot] = true;
+    }
+    kache_b200::Pinned_Buf& buf = stage[st.slot];
+    buf.ensure(bytes + 64);
+    char* base = buf.as<char>();
+    std::vector<uint64_t> off(n + 1, 0);
+    for(size_t q = 0; q < n; ++q)
+        off[q + 1] = off[q] + st.lens[q];
+    st.seqs.resize(n);
+    std::vector<const char*> src;
+    src.reserve(n);
+    for(const Request* r : g)
+        src.insert(src.end(), r->seqs.begin(), r->seqs.end());
+    kache_b200::parallel_for(n, 2048, [&](const size_t s, const size_t e)
+    {
+        for(size_t q = s; q < e; ++q)
+        {
+            st.seqs[q] = base + off[q];
+            if(st.lens[q])
+                std::memcpy(base + off[q], src[q], st.lens[q]);
+        }
+    });
+}
+
+// The executor: runs the staged runs on the GPU in the order they were formed.
+void kache_server::execute()
+{
+    for(;;)
+    {
+        Staged* st = nullptr;
+        {
+            std::unique_lock<std::mutex> lk(mu);
+            ready_cv.wait(lk, [&](){ return staging_done || !ready.empty(); });
+            if(ready.empty())
+                return;
+            st = ready.front();
+            ready.pop_front();
+        }
+        run(*st);
+        {
+            std::lock_guard<std::mutex> lk(mu);
+            const auto now = clock_type::now();
+            for(Request* r : st->g)
+                r->done = true, r->t_done = now;
+            runs++, merged += st->g.size();
+            if(st->slot >= 0)
+                slot_busy[st->slot] = false;
+        }
+        done_cv.notify_all();
+        ready_cv.notify_all();
+        delete st;
+    }
+}
+
+void kache_server::run(Staged& st)
+{
+    const auto& g = st.g;
+    const auto& seqs = st.seqs;
+    const auto& lens = st.lens;
+    const auto& first = st.first;
+    const auto& pos_first = st.pos_first;
     const size_t n = seqs.size();
     const Request& h = *g.front();
     const size_t vb = t->value_bytes;
@@ -243,6 +346,9 @@ extern "C" int kache_b200_server_new(kache_table* const t, const uint64_t budget
         const uint64_t P = kache_server::run_positions;
         s->found.ensure(P + 16), s->values.ensure(P * std::max<uint32_t>(1, t->value_bytes) + 16);
         s->counts.ensure((P / 16) * 8);
+        // Staging for the bases of a full-size run of reads of 100 bp or more (positions x 1.5), in both buffers.
+        s->stage[0].ensure(P * 3 / 2), s->stage[1].ensure(P * 3 / 2);
+        s->executor = std::thread([s](){ s->execute(); });
         s->worker = std::thread([s](){ s->loop(); });
         *out = s;
         return KACHE_OK;
@@ -268,6 +374,8 @@ extern "C" void kache_b200_server_free(kache_server* const s) noexcept
     s->cv.notify_all();
     if(s->worker.joinable())
         s->worker.join();
+    if(s->executor.joinable())
+        s->executor.join();
     for(auto& kv : s->all)
         delete kv.second;
     delete s;

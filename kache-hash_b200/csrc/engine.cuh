@@ -655,6 +655,8 @@ class Engine final : public kache_table
             check(cudaMemcpyAsync(d + o_off, off, (n + 1) * 8, cudaMemcpyHostToDevice, stream_), "H2D offsets");
             return stage_dev(reinterpret_cast<const uint8_t*>(d), reinterpret_cast<const uint64_t*>(d + o_off), n, lanes);
         }
+        if(n >= host_list_max)
+            return stage_gathered(seqs, lens, n, bytes, lanes);
         const uint32_t seg_len = seg_len_for(lanes, max_pos, all_pos);
         uint64_t nsegs = 0;
         for(size_t i = 0; i < n; ++i)
@@ -720,6 +722,45 @@ class Engine final : public kache_table
                          reinterpret_cast<const uint64_t*>(d + o_seg), reinterpret_cast<const uint64_t*>(d + o_pos), n, nsegs, seg_len};
         bi.total_pos = p;
         return bi;
+    }
+
+    // Pageable batches of many sequences: gathered end to end into page-locked memory in pieces, each piece's copy to
+    // the device overlapping the next piece's gather, then listed on the device as a page-locked batch is. Listing a
+    // million reads on the host (three passes and a counting sort) would take longer than the kernel that follows.
+    static constexpr size_t host_list_max = 16384;
+
+    Batch_Info stage_gathered(const char* const* seqs, const size_t* lens, const size_t n, const uint64_t bytes, const bool lanes)
+    {
+        const size_t o_hb = (n + 1) * 8;
+        pin_.ensure(o_hb + bytes + 64);
+        auto* off = pin_.as<uint64_t>();
+        char* hb = pin_.as<char>(o_hb);
+        uint64_t b = 0;
+        for(size_t i = 0; i < n; ++i)
+            off[i] = b, b += lens[i];
+        off[n] = b;
+        const size_t o_off = (bytes + 64 + 15) / 16 * 16;
+        dhost_.ensure(o_off + (n + 1) * 8);
+        char* d = dhost_.as<char>();
+        check(cudaMemcpyAsync(d + o_off, off, (n + 1) * 8, cudaMemcpyHostToDevice, stream_), "H2D offsets");
+        constexpr uint64_t piece = uint64_t(16) << 20;
+        for(size_t i0 = 0; i0 < n; )
+        {
+            size_t i1 = i0;
+            while(i1 < n && off[i1] - off[i0] < piece)
+                i1++;
+            parallel_for(i1 - i0, 2048, [&](const size_t s, const size_t e)
+            {
+                for(size_t i = i0 + s; i < i0 + e; ++i)
+                    if(lens[i])
+                        std::memcpy(hb + off[i], seqs[i], lens[i]);
+            });
+            if(off[i1] > off[i0])
+                check(cudaMemcpyAsync(d + off[i0], hb + off[i0], off[i1] - off[i0], cudaMemcpyHostToDevice, stream_), "H2D batch");
+            i0 = i1;
+        }
+        check(cudaMemsetAsync(d + bytes, 0, 64, stream_), "memset");
+        return stage_dev(reinterpret_cast<const uint8_t*>(d), reinterpret_cast<const uint64_t*>(d + o_off), n, lanes);
     }
 
     // stage_dev for a batch of at most small_stage_max sequences: one block counts and sums, one kernel lists.

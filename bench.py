@@ -762,9 +762,43 @@ def run_config5(args):
 
     dev_ms = timed_steps(stream, dev_step, 3, 1)
     T.set_stream(None)
-    del dreq, runs_dev
+    del runs_dev
+    torch.cuda.synchronize()
 
     S = kache.Server(T)
+
+    def serve_dev(arrivals=None):
+        """The same requests resident in HBM submitted to the server from four threads, at once or at `arrivals`
+        seconds: runs of device requests are kache_b200_run_dev_batches calls. Returns wall seconds and latencies."""
+        tickets = [None] * len(dreq)
+        start = time.perf_counter()
+
+        def client(idx):
+            for i in idx:
+                if arrivals is not None:
+                    delay = start + arrivals[i] - time.perf_counter()
+                    if delay > 0:
+                        time.sleep(delay)
+                kind, db, do, n_, o0, o1 = dreq[i]
+                tickets[i] = S.submit_dev(kind, db.data_ptr(), do.data_ptr(), n_, op=kache.ADD, x=1, init=1,
+                                          out0=None if o0 is None else o0.data_ptr(), out1=None if o1 is None else o1.data_ptr())
+
+        th = [threading.Thread(target=client, args=(range(j, len(dreq), 4),)) for j in range(4)]
+        for t in th:
+            t.start()
+        for t in th:
+            t.join()
+        lat = [S.wait(t)[1] for t in tickets]
+        return time.perf_counter() - start, np.array(lat)
+
+    serve_dev()     # warm-up
+    rd0, _ = S.stats()
+    dev_served_s, dev_served_lat = serve_dev()
+    rd1, _ = S.stats()
+    dev_rate = 0.6 * len(dreq) / dev_served_s
+    dev_open_s, dev_open_lat = serve_dev(np.cumsum(rng.exponential(1.0 / dev_rate, size=len(dreq))))
+    rd2, _ = S.stats()
+    del dreq
 
     def serve(arrivals):
         """Submits request i at arrivals[i] seconds (all at once if None) from four threads; returns wall seconds and
@@ -813,6 +847,13 @@ def run_config5(args):
                        "batched_device": {"value": P / (dev_ms * 1e-3), "ms": dev_ms, "calls": 3,
                                           "form": "kache_b200_run_dev_batches per kind, requests resident in HBM",
                                           "served_burst_fraction": dev_ms * 1e-3 / burst_s},
+                       "served_device_burst": {"value": P / dev_served_s, "ms": 1000 * dev_served_s,
+                                               "p50_ms": pct(dev_served_lat, 50), "p99_ms": pct(dev_served_lat, 99),
+                                               "runs": rd1 - rd0, "requests": len(reqs),
+                                               "fraction_of_batched_device": dev_ms * 1e-3 / dev_served_s,
+                                               "form": "the requests resident in HBM, submitted to the server at once from four threads"},
+                       "served_device_poisson": {"offered_requests_per_s": dev_rate, "value": P / dev_open_s,
+                                                 "p50_ms": pct(dev_open_lat, 50), "p99_ms": pct(dev_open_lat, 99), "runs": rd2 - rd1},
                        "served_burst": {"value": P / burst_s, "p50_ms": pct(burst_lat, 50), "p99_ms": pct(burst_lat, 99),
                                         "runs": runs1 - runs0, "requests": len(reqs)},
                        "served_poisson": {"offered_requests_per_s": rate, "value": P / open_s, "p50_ms": pct(open_lat, 50),

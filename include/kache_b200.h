@@ -53,7 +53,8 @@ int kache_b200_count_dev(kache_table* t, const uint8_t* d_bases, const uint64_t*
  * arrays and results. Each sequence is read where its batch holds it; nothing is copied. kind is one of
  * KACHE_B200_RUN_*; op, x and y are the operation and its operands (upsert: x and init; oriented upsert: x_fwd and
  * x_rev; update: x). Per batch, `result` is set to the keys it inserted (upserts; a key that two batches of the call
- * insert is credited to one of them) or the k-mers of it present (update), and to 0 otherwise. Lookups write each
+ * insert is credited to one of them), the k-mers of it present (update), its positions found (lookup: found flags
+ * equal to 1) or the sum of its per-sequence counts (count). Lookups write each
  * batch's found flags, values and orientations to its out0, out1, out2 (device arrays laid out as kache_lookup's;
  * out1 and out2 may be NULL); counts write its per-sequence counts to out0 (a device array of n uint64_t). The call
  * returns synchronised with the table's stream. */
@@ -131,6 +132,13 @@ typedef struct kache_server kache_server;
 int kache_b200_server_new(kache_table* t, uint64_t budget_bytes, kache_server** out) KACHE_NOEXCEPT;
 void kache_b200_server_free(kache_server* s) KACHE_NOEXCEPT;
 int kache_b200_server_submit(kache_server* s, uint32_t kind, const char* const* seqs, const size_t* lens, size_t n, uint32_t op, uint64_t x, uint64_t init, void* out0, void* out1, void* out2, uint64_t* ticket) KACHE_NOEXCEPT;
+/* A request whose sequences and outputs are already in device memory, laid out as kache_b200_run_dev_batches's
+ * batches: sequence i is d_bases[d_off[i], d_off[i + 1]), outputs out0..2 are device arrays as kache_b200_server_submit
+ * takes them. The arrays must hold their data when submitted (the work writing them finished) and stay valid until
+ * kache_b200_server_wait returns for it. Device requests merge only with device requests of the same kind (and, for
+ * upserts, op, x and init), into one kache_b200_run_dev_batches call: nothing is gathered or copied on the host. Their
+ * results are those of host requests: keys inserted, positions found, or the sum of the counts. */
+int kache_b200_server_submit_dev(kache_server* s, uint32_t kind, const uint8_t* d_bases, const uint64_t* d_off, uint64_t n, uint32_t op, uint64_t x, uint64_t init, void* out0, void* out1, void* out2, uint64_t* ticket) KACHE_NOEXCEPT;
 /* Waits for a request; its result at *result, the time from its submission to its completion at *latency_ms. */
 int kache_b200_server_wait(kache_server* s, uint64_t ticket, uint64_t* result, double* latency_ms) KACHE_NOEXCEPT;
 /* Merged runs so far, and the requests they ran. */

@@ -462,4 +462,42 @@ static __global__ void batches_scatter_kernel(const uint64_t* desc, const unsign
     }
 }
 
+// Per-batch present positions of a lookup of several batches: each thread counts the found flags equal to 1 over
+// chunks of 64 merged positions, read from the batch's own array (desc word 4) and flushed at batch changes.
+// pos_base[b] is batch b's first merged position (non-decreasing in b); P is the merged positions.
+static __global__ void batches_hits_kernel(const uint64_t* desc, const uint64_t* pos_base, const uint64_t count,
+                                           const uint64_t P, unsigned long long* per_batch)
+{
+    const uint64_t chunks = (P + 63) / 64, stride = uint64_t(gridDim.x) * blockDim.x;
+    for(uint64_t c = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; c < chunks; c += stride)
+    {
+        const uint64_t p0 = c * 64, p1 = min(P, p0 + 64);
+        uint64_t lo = 0, hi = count;    // The first batch starting past p0; the one before it holds p0.
+        while(lo < hi)
+        {
+            const uint64_t mid = (lo + hi) / 2;
+            if(pos_base[mid] <= p0)
+                lo = mid + 1;
+            else
+                hi = mid;
+        }
+        uint64_t b = lo - 1;
+        uint64_t end = b + 1 < count ? pos_base[b + 1] : P;
+        unsigned long long acc = 0;
+        for(uint64_t p = p0; p < p1; ++p)
+        {
+            while(p >= end)
+            {
+                if(acc)
+                    atomicAdd(per_batch + b, acc), acc = 0;
+                ++b;
+                end = b + 1 < count ? pos_base[b + 1] : P;
+            }
+            acc += reinterpret_cast<const uint8_t*>(desc[8 * b + 4])[p - pos_base[b]] == 1;
+        }
+        if(acc)
+            atomicAdd(per_batch + b, acc);
+    }
+}
+
 }

@@ -1435,7 +1435,6 @@ public:
         bi.b.seq_addr = addr;
         dout_.ensure(N * 8 + 8);
         auto* per_seq = dout_.as<unsigned long long>();
-        const bool sums = kind != KACHE_B200_RUN_LOOKUP && kind != KACHE_B200_RUN_COUNT;
         if(kind != KACHE_B200_RUN_LOOKUP)
             check(cudaMemsetAsync(per_seq, 0, N * 8, stream_), "memset");
         if(kind == KACHE_B200_RUN_UPSERT)
@@ -1466,18 +1465,18 @@ public:
             Lookup_Batches_Visitor<set_, VT> vis{{T_, bi.b.pos_off, nullptr, nullptr, nullptr, 0}, batch_of, desc, pos_base};
             stream_launch(K_LOOKUP, bi, 0, bi.b.nsegs, vis, true);
         }
-        if(sums)
-        {
-            check(cudaMemsetAsync(res, 0, count * 8, stream_), "memset");
+        // Per-batch results: the per-sequence counters summed per batch (keys inserted, k-mers present, counts), or
+        // a lookup's found flags equal to 1 counted per batch.
+        check(cudaMemsetAsync(res, 0, count * 8, stream_), "memset");
+        if(kind != KACHE_B200_RUN_LOOKUP)
             launch(K_OTHER, [&](){ batches_sum_kernel<<<grid_for((N + 31) / 32 / 64 + 1, 8), 256, 0, stream_>>>(per_seq, batch_of, N, res); });
-            auto* hr = pin_multi_.as<uint64_t>();
-            check(cudaMemcpyAsync(hr, res, count * 8, cudaMemcpyDeviceToHost, stream_), "D2H results");
-            sync();
-            for(size_t b = 0; b < count; ++b)
-                bs[b].result = hr[b];
-        }
-        else
-            sync();
+        else if(bi.total_pos > 0)
+            launch(K_OTHER, [&](){ batches_hits_kernel<<<grid_for((bi.total_pos + 63) / 64 / 32 + 1, 8), 256, 0, stream_>>>(desc, pos_base, count, bi.total_pos, res); });
+        auto* hr = pin_multi_.as<uint64_t>();
+        check(cudaMemcpyAsync(hr, res, count * 8, cudaMemcpyDeviceToHost, stream_), "D2H results");
+        sync();
+        for(size_t b = 0; b < count; ++b)
+            bs[b].result = hr[b];
         if(lanes)
             finish_tune();
     }

@@ -11,6 +11,8 @@
 // (device memory for the merged batch), so a burst of requests waits rather than exhausting HBM. Two threads share the
 // work: a stager forms the next run and gathers its reads end to end into one of two page-locked buffers while an
 // executor runs the run before it on the GPU and copies its results out, so the host's copying overlaps the device.
+// Requests whose reads and outputs are already in device memory (kache_b200_server_submit_dev) merge with each other
+// into one call of the several-batches form (kache_b200_run_dev_batches): nothing to gather, nothing to copy out.
 #include "engine.cuh"
 #include "kache_b200.h"
 
@@ -38,6 +40,12 @@ struct Request
     void* out0;                     // lookup: found; count: counts
     void* out1;                     // lookup: values (or null)
     void* out2;                     // lookup: fwd (or null)
+    // A device request (kache_b200_server_submit_dev): its n sequences are d_bases[d_off[i], d_off[i + 1]) and its
+    // outputs out0..2 are device arrays; seqs and lens stay empty.
+    bool dev = false;
+    const uint8_t* d_bases = nullptr;
+    const uint64_t* d_off = nullptr;
+    uint64_t n_dev = 0;
     uint64_t positions = 0, bytes = 0, result = 0;
     int status = KACHE_OK;
     bool done = false;
@@ -67,6 +75,9 @@ struct kache_server
     // Most k-mer positions of one merged run (unless its first request alone has more): enough to keep every SM
     // busy, few enough that a run's staging buffers stay reused and a request waits behind one run at most this big.
     static constexpr uint64_t run_positions = uint64_t(1) << 24;
+    // The same for runs of device requests, bounded by bases: they stage nothing on the host, so a run costs only its
+    // fixed per-call steps and fewer, larger runs keep the GPU busier; 2^26 bases take a few milliseconds.
+    static constexpr uint64_t dev_run_positions = uint64_t(1) << 26;
     // Most bases of a run gathered into a staging buffer; larger runs are handed over from the callers' memory.
     static constexpr uint64_t stage_max = uint64_t(256) << 20;
     std::mutex mu;
@@ -85,6 +96,11 @@ struct kache_server
     // Merged outputs, reused across runs, in page-locked memory (the table copies into it directly).
     kache_b200::Pinned_Buf found, fwd, values, counts;
     uint64_t runs = 0, merged = 0;
+    // For device requests: a stream of the server's own (not ordered with the table's work) and a page-locked word
+    // pair on which a submission reads its batch's first and last offsets, under probe_mu.
+    cudaStream_t probe = nullptr;
+    kache_b200::Pinned_Buf probe_buf;
+    std::mutex probe_mu;
 
     void loop();
     void execute();
@@ -107,11 +123,11 @@ uint64_t request_bytes(const Request& r, const uint32_t k, const uint32_t vb)
 
 bool compatible(const Request& a, const Request& b)
 {
-    if(a.kind != b.kind)
+    if(a.kind != b.kind || a.dev != b.dev)
         return false;
     if(a.kind == KACHE_B200_REQ_UPSERT)
         return a.op == b.op && a.x == b.x && a.init == b.init;
-    if(a.kind == KACHE_B200_REQ_LOOKUP)
+    if(a.kind == KACHE_B200_REQ_LOOKUP && !a.dev)     // Device lookups bind their own output arrays per request.
         return (a.out1 == nullptr) == (b.out1 == nullptr) && (a.out2 == nullptr) == (b.out2 == nullptr);
     return true;
 }
@@ -125,7 +141,9 @@ void kache_server::loop()
         std::vector<Request*> g;
         {
             std::unique_lock<std::mutex> lk(mu);
-            cv.wait(lk, [&](){ return stop || !queue.empty(); });
+            // The next run is formed once the executor has taken the one before it, so requests arriving meanwhile
+            // merge into it instead of queueing as runs of their own.
+            cv.wait(lk, [&](){ return stop || (!queue.empty() && ready.empty()); });
             if(queue.empty())
             {
                 staging_done = true;
@@ -138,7 +156,8 @@ void kache_server::loop()
             uint64_t bytes = 0, pos = 0;
             std::deque<Request*> rest;
             for(Request* r : queue)
-                if(g.empty() || (compatible(*r, *g.front()) && bytes + r->bytes <= budget && pos + r->positions <= run_positions))
+                if(g.empty() || (compatible(*r, *g.front()) && bytes + r->bytes <= budget &&
+                                 pos + r->positions <= (r->dev ? dev_run_positions : run_positions)))
                     bytes += r->bytes, pos += r->positions, g.push_back(r);
                 else
                     rest.push_back(r);
@@ -160,6 +179,8 @@ void kache_server::loop()
 void kache_server::gather(Staged& st)
 {
     const auto& g = st.g;
+    if(g.front()->dev)
+        return;     // Device requests are read where they lie.
     st.first.assign(g.size() + 1, 0), st.pos_first.assign(g.size() + 1, 0);
     uint64_t bytes = 0;
     for(size_t i = 0; i < g.size(); ++i)
@@ -219,6 +240,7 @@ void kache_server::execute()
             st = ready.front();
             ready.pop_front();
         }
+        cv.notify_all();    // The stager may form the next run.
         run(*st);
         {
             std::lock_guard<std::mutex> lk(mu);
@@ -247,7 +269,20 @@ void kache_server::run(Staged& st)
     const size_t vb = t->value_bytes;
     try
     {
-        if(h.kind == KACHE_B200_REQ_UPSERT)
+        if(h.dev)
+        {
+            // One call of the several-batches form over the requests' device batches; each request's outputs go
+            // straight to its own device arrays and its result comes back per batch.
+            std::vector<kache_dev_batch> bs(g.size());
+            for(size_t i = 0; i < g.size(); ++i)
+                bs[i] = kache_dev_batch{g[i]->d_bases, g[i]->d_off, g[i]->n_dev, g[i]->out0, g[i]->out1, g[i]->out2, 0};
+            const uint32_t kind = h.kind == KACHE_B200_REQ_UPSERT ? KACHE_B200_RUN_UPSERT
+                                : h.kind == KACHE_B200_REQ_LOOKUP ? KACHE_B200_RUN_LOOKUP : KACHE_B200_RUN_COUNT;
+            t->run_dev_batches(user, kind, h.op, h.x, h.init, bs.data(), bs.size());
+            for(size_t i = 0; i < g.size(); ++i)
+                g[i]->result = bs[i].result;
+        }
+        else if(h.kind == KACHE_B200_REQ_UPSERT)
         {
             counts.ensure((n + 1) * 8);
             const uint64_t* c = counts.as<uint64_t>();
@@ -348,6 +383,12 @@ extern "C" int kache_b200_server_new(kache_table* const t, const uint64_t budget
         s->counts.ensure((P / 16) * 8);
         // Staging for the bases of a full-size run of reads of 100 bp or more (positions x 1.5), in both buffers.
         s->stage[0].ensure(P * 3 / 2), s->stage[1].ensure(P * 3 / 2);
+        if(cudaStreamCreateWithFlags(&s->probe, cudaStreamNonBlocking) != cudaSuccess)
+        {
+            delete s;
+            return KACHE_EINTERNAL;
+        }
+        s->probe_buf.ensure(16);
         s->executor = std::thread([s](){ s->execute(); });
         s->worker = std::thread([s](){ s->loop(); });
         *out = s;
@@ -378,6 +419,8 @@ extern "C" void kache_b200_server_free(kache_server* const s) noexcept
         s->executor.join();
     for(auto& kv : s->all)
         delete kv.second;
+    if(s->probe)
+        cudaStreamDestroy(s->probe);
     delete s;
 }
 
@@ -400,6 +443,65 @@ extern "C" int kache_b200_server_submit(kache_server* const s, const uint32_t ki
         for(const size_t len : r->lens)
             r->positions += len >= k ? len - k + 1 : 0;
         r->bytes = request_bytes(*r, k, s->t->value_bytes);
+        r->t_submit = clock_type::now();
+        {
+            std::lock_guard<std::mutex> lk(s->mu);
+            r->ticket = s->next_ticket++;
+            s->all[r->ticket] = r;
+            s->queue.push_back(r);
+        }
+        s->cv.notify_one();
+        *ticket = r->ticket;
+        return KACHE_OK;
+    }
+    catch(const std::bad_alloc&)
+    {
+        return KACHE_ENOMEM;
+    }
+}
+
+extern "C" int kache_b200_server_submit_dev(kache_server* const s, const uint32_t kind, const uint8_t* const d_bases, const uint64_t* const d_off,
+                                            const uint64_t n, const uint32_t op, const uint64_t x, const uint64_t init, void* const out0,
+                                            void* const out1, void* const out2, uint64_t* const ticket) noexcept
+{
+    if(s == nullptr || ticket == nullptr || kind > KACHE_B200_REQ_COUNT || (n > 0 && (d_bases == nullptr || d_off == nullptr)))
+        return KACHE_EINVAL;
+    if(kind != KACHE_B200_REQ_UPSERT && n > 0 && out0 == nullptr)
+        return KACHE_EINVAL;
+    if(kind == KACHE_B200_REQ_UPSERT && op != KACHE_B200_ADD_WRAP && op > KACHE_MAX)
+        return KACHE_EINVAL;
+    if(kind == KACHE_B200_REQ_LOOKUP && s->t->value_bytes == 0 && out1 != nullptr)
+        return KACHE_EINVAL;
+    try
+    {
+        auto* r = new Request;
+        r->kind = kind, r->op = op, r->x = x, r->init = init, r->out0 = out0, r->out1 = out1, r->out2 = out2;
+        r->dev = true, r->d_bases = d_bases, r->d_off = d_off, r->n_dev = n;
+        // The batch's bases bound its positions: read its first and last offsets (a 16-byte copy on the server's
+        // own stream, so a submission never waits for the table's work).
+        uint64_t bases = 0;
+        if(n > 0)
+        {
+            std::lock_guard<std::mutex> lk(s->probe_mu);
+            uint64_t* h = s->probe_buf.as<uint64_t>();
+            if(cudaMemcpyAsync(h, d_off, 8, cudaMemcpyDeviceToHost, s->probe) != cudaSuccess ||
+               cudaMemcpyAsync(h + 1, d_off + n, 8, cudaMemcpyDeviceToHost, s->probe) != cudaSuccess ||
+               cudaStreamSynchronize(s->probe) != cudaSuccess)
+            {
+                delete r;
+                return KACHE_EINTERNAL;
+            }
+            if(h[1] < h[0])
+            {
+                delete r;
+                return KACHE_EINVAL;
+            }
+            bases = h[1] - h[0];
+        }
+        r->positions = bases;
+        // Device bytes of its share of the merged list: offsets, addresses, lengths, per-sequence results and batch
+        // numbers (36 bytes a sequence), and segment entries (8 bytes per 16 positions at most).
+        r->bytes = 36 * n + bases / 2 + 64;
         r->t_submit = clock_type::now();
         {
             std::lock_guard<std::mutex> lk(s->mu);

@@ -103,6 +103,7 @@ def lib():
             "kache_b200_server_new": (ctypes.c_int, [_vp, ctypes.c_uint64, ctypes.POINTER(_vp)]),
             "kache_b200_server_free": (None, [_vp]),
             "kache_b200_server_submit": (ctypes.c_int, [_vp, ctypes.c_uint32, _vp, _vp, ctypes.c_size_t, ctypes.c_uint32, ctypes.c_uint64, ctypes.c_uint64, _vp, _vp, _vp, _u64p]),
+            "kache_b200_server_submit_dev": (ctypes.c_int, [_vp, ctypes.c_uint32, _vp, _vp, ctypes.c_uint64, ctypes.c_uint32, ctypes.c_uint64, ctypes.c_uint64, _vp, _vp, _vp, _u64p]),
             "kache_b200_server_wait": (ctypes.c_int, [_vp, ctypes.c_uint64, _u64p, ctypes.POINTER(ctypes.c_double)]),
             "kache_b200_server_stats": (ctypes.c_int, [_vp, _u64p, _u64p]),
             "kache_b200_memory_roof": (ctypes.c_int, [ctypes.c_uint64, ctypes.c_uint32, ctypes.c_uint64, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)]),
@@ -326,7 +327,7 @@ class Table:
 
     def run_dev_batches(self, kind, batches, op=0, x=0, y=0, user=0):
         """Runs device batches as one call (kache_b200_run_dev_batches). `batches` holds tuples (d_bases, d_off, n[,
-        out0[, out1[, out2]]]) of device pointers; returns each batch's result (keys inserted, k-mers present, or 0)."""
+        out0[, out1[, out2]]]) of device pointers; returns each batch's result (keys inserted, k-mers present, positions found, or the sum of its counts)."""
         arr = (DevBatch * max(1, len(batches)))()
         for i, b in enumerate(batches):
             outs = list(b[3:]) + [None] * (6 - len(b))
@@ -440,6 +441,15 @@ class Server:
         _check(lib().kache_b200_server_submit(self.h, kind, *b.args(), op, x, init, _p(out0), _p(out1), _p(out2), ctypes.byref(t)),
                "kache_b200_server_submit")
         self.keep[t.value] = (b, out0, out1, out2)    # The request's buffers live until it completes.
+        return t.value
+
+    def submit_dev(self, kind, d_bases, d_off, n, op=0, x=0, init=0, out0=None, out1=None, out2=None, keep=None):
+        """A request resident in device memory (kache_b200_server_submit_dev): device addresses of the bases, the n + 1
+        offsets and the outputs; `keep` holds whatever owns them until the request completes."""
+        t = ctypes.c_uint64()
+        _check(lib().kache_b200_server_submit_dev(self.h, kind, d_bases, d_off, n, op, x, init, out0, out1, out2, ctypes.byref(t)),
+               "kache_b200_server_submit_dev")
+        self.keep[t.value] = keep
         return t.value
 
     def wait(self, ticket):

@@ -2,8 +2,8 @@
 
 Each kind of the call is checked bit-exact: upserts (the table's dump, size, capacity and the sum of the per-batch
 inserted counts; per batch exact where the batches share no k-mer), oriented upserts, present-only updates (per-batch
-present counts and the final table), per-position lookups (each batch's own found, value and orientation arrays) and
-per-sequence counts (each batch's own array). The batches are ragged: empty batches, batches without a k-mer,
+present counts and the final table), per-position lookups (each batch's own found, value and orientation arrays, and
+its positions found) and per-sequence counts (each batch's own array, and their sum). The batches are ragged: empty batches, batches without a k-mer,
 sequences shorter than k, non-ACGT characters, lowercase runs, offsets that do not start at 0 (a batch that is a
 window of a larger buffer), more sequences than one block sums, and more batches than one block lists.
 """
@@ -87,22 +87,23 @@ def test_upsert_lookup_count_update(vb):
         P = max(1, _positions(b))
         outs.append((torch.full((P,), 7, dtype=torch.uint8, device=dev), torch.zeros(P * vb, dtype=torch.uint8, device=dev),
                      torch.full((P,), 7, dtype=torch.uint8, device=dev)))
-    G.run_dev_batches(kache.RUN_LOOKUP, [(b.data_ptr(), o.data_ptr(), n, f.data_ptr(), v.data_ptr(), w.data_ptr())
-                                          for (b, o, n), (f, v, w) in zip(devb, outs)])
+    hits = G.run_dev_batches(kache.RUN_LOOKUP, [(b.data_ptr(), o.data_ptr(), n, f.data_ptr(), v.data_ptr(), w.data_ptr())
+                                                 for (b, o, n), (f, v, w) in zip(devb, outs)])
     dt = {8: np.uint64, 4: np.uint32, 1: np.uint8}[vb]
-    for hb, (f, v, w) in zip(host, outs):
+    for hb, (f, v, w), h in zip(host, outs, hits):
         P = _positions(hb)
         fo, vo_, wo = O.lookup(hb)
+        assert h == int((fo == 1).sum())
         assert np.array_equal(f.cpu().numpy()[:P], fo)
         assert np.array_equal(v.cpu().numpy().view(dt)[:P], vo_.astype(dt))
         assert np.array_equal(w.cpu().numpy()[:P], wo)
 
     # Per-sequence counts into each batch's array.
     counts = [torch.full((max(1, n),), 99, dtype=torch.int64, device=dev) for _, _, n in devb]
-    assert G.run_dev_batches(kache.RUN_COUNT, [(b.data_ptr(), o.data_ptr(), n, c.data_ptr()) for (b, o, n), c in zip(devb, counts)]) \
-        == [0] * len(devb)
-    for hb, c in zip(host, counts):
+    sums = G.run_dev_batches(kache.RUN_COUNT, [(b.data_ptr(), o.data_ptr(), n, c.data_ptr()) for (b, o, n), c in zip(devb, counts)])
+    for hb, c, sm in zip(host, counts, sums):
         assert np.array_equal(c.cpu().numpy().view(np.uint64)[:hb.n], O.count(hb))
+        assert sm == int(O.count(hb).sum())
 
     # Present-only update: per-batch present counts, then the same table.
     res = G.run_dev_batches(kache.RUN_UPDATE, [(b.data_ptr(), o.data_ptr(), n) for b, o, n in devb], kache.ADD_WRAP, 3)
@@ -164,10 +165,12 @@ def test_oriented_and_set():
     assert np.array_equal(S.dump()[0], SO.dump()[0])
     dev = torch.device("cuda", 0)
     found = [torch.full((max(1, int(b.positions(32).sum())),), 7, dtype=torch.uint8, device=dev) for b in host]
-    S.run_dev_batches(kache.RUN_LOOKUP, [(b.data_ptr(), o.data_ptr(), n, f.data_ptr()) for (b, o, n), f in zip(devb, found)])
-    for hb, f in zip(host, found):
+    hits = S.run_dev_batches(kache.RUN_LOOKUP, [(b.data_ptr(), o.data_ptr(), n, f.data_ptr()) for (b, o, n), f in zip(devb, found)])
+    for hb, f, h in zip(host, found, hits):
         P = int(hb.positions(32).sum())
-        assert np.array_equal(f.cpu().numpy()[:P], SO.lookup(hb)[0])
+        fo = SO.lookup(hb)[0]
+        assert np.array_equal(f.cpu().numpy()[:P], fo)
+        assert h == int((fo == 1).sum())
     S.close()
 
 

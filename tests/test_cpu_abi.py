@@ -76,6 +76,9 @@ def test_null_table_and_strerror():
     assert L.kache_size(None, None) == kache.KACHE_EINVAL
     assert L.kache_get_stats(None, None) == kache.KACHE_EINVAL
     assert L.kache_b200_clear(None) == kache.KACHE_EINVAL
+    t = ctypes.c_uint64()
+    assert L.kache_b200_server_submit(None, 0, None, None, 0, 0, 0, 0, None, None, None, ctypes.byref(t)) == kache.KACHE_EINVAL
+    assert L.kache_b200_server_submit_dev(None, 0, None, None, 0, 0, 0, 0, None, None, None, ctypes.byref(t)) == kache.KACHE_EINVAL
     names = {0: b"success", 1: b"invalid argument", 2: b"too many users registered", 3: b"out of memory", 4: b"internal error", 9: b"unknown status"}
     for c, s in names.items():
         assert L.kache_strerror(c) == s

@@ -961,6 +961,23 @@ class Engine final : public kache_table
         return c;
     }
 
+    // The bucket count to rebuild a non-empty table at when the schedule needs `target`: one doubling more while the
+    // wider arrays take at most half the device memory free (counting the spare arrays a rebuild reuses), so that a
+    // table growing call after call is rebuilt at every other doubling of its capacity, moving about a third fewer
+    // keys over all its rebuilds (each of which rehashes every key it moves). Where keys sit is not observable; the
+    // capacity reported stays the schedule's.
+    uint64_t rebuild_cap(const uint64_t target)
+    {
+        const uint64_t wide = 2 * target;
+        if(wide > max_buckets)
+            return target;
+        const size_t need = wide * (B + 32 + B * slot_bytes) + ov_slots_for(std::max<uint64_t>(1024, wide)) * 32;
+        size_t free_b = 0, total_b = 0;
+        check(cudaMemGetInfo(&free_b, &total_b), "cudaMemGetInfo");
+        const size_t spare = cs2_.bytes + spill2_.bytes + slots2_.bytes + ov2_.bytes;
+        return 2 * need <= free_b + spare ? wide : target;
+    }
+
     // Grows the device table to `target` buckets ahead of a call's inserts: where keys sit is not observable, so the
     // device table may have more buckets than the capacity the schedule reports, never fewer. An empty table is
     // reallocated and zeroed rather than rebuilt. Skipped if the arrays would not fit in free device memory.
@@ -982,7 +999,7 @@ class Engine final : public kache_table
         }
         if(size_ != 0)
         {
-            resize(target);
+            resize(rebuild_cap(target));
             return;
         }
         alloc_table(cs_, spill_, slots_, target);
@@ -1055,7 +1072,7 @@ class Engine final : public kache_table
             size_ += ins, total_ins += ins;
             acct.add(ins);
             if(cap_ > T_.cap)
-                resize(cap_);
+                resize(rebuild_cap(cap_));
             if(c[1] * 4 > ov_slots_ * 3)
                 grow_overflow();
             sb = se;

@@ -75,9 +75,10 @@ struct kache_server
     // Most k-mer positions of one merged run (unless its first request alone has more): enough to keep every SM
     // busy, few enough that a run's staging buffers stay reused and a request waits behind one run at most this big.
     static constexpr uint64_t run_positions = uint64_t(1) << 24;
-    // The same for runs of device requests, bounded by bases: they stage nothing on the host, so a run costs only its
-    // fixed per-call steps and fewer, larger runs keep the GPU busier; 2^26 bases take a few milliseconds.
-    static constexpr uint64_t dev_run_positions = uint64_t(1) << 26;
+    // Most sequences of one run of device requests (unless its first request alone has more). Their lengths lie in
+    // device memory, unread by the host; they stage nothing on the host, so a run costs only its fixed per-call steps,
+    // and fewer, larger runs keep the GPU busier: 2^20 short reads take a few milliseconds.
+    static constexpr uint64_t dev_run_seqs = uint64_t(1) << 20;
     // Most bases of a run gathered into a staging buffer; larger runs are handed over from the callers' memory.
     static constexpr uint64_t stage_max = uint64_t(256) << 20;
     std::mutex mu;
@@ -96,11 +97,6 @@ struct kache_server
     // Merged outputs, reused across runs, in page-locked memory (the table copies into it directly).
     kache_b200::Pinned_Buf found, fwd, values, counts;
     uint64_t runs = 0, merged = 0;
-    // For device requests: a stream of the server's own (not ordered with the table's work) and a page-locked word
-    // pair on which a submission reads its batch's first and last offsets, under probe_mu.
-    cudaStream_t probe = nullptr;
-    kache_b200::Pinned_Buf probe_buf;
-    std::mutex probe_mu;
 
     void loop();
     void execute();
@@ -153,12 +149,12 @@ void kache_server::loop()
             }
             // The run: the head, then every waiting request that can merge with it, in arrival order, within budget;
             // the others keep their order in the queue.
-            uint64_t bytes = 0, pos = 0;
+            uint64_t bytes = 0, pos = 0, seqs = 0;
             std::deque<Request*> rest;
             for(Request* r : queue)
                 if(g.empty() || (compatible(*r, *g.front()) && bytes + r->bytes <= budget &&
-                                 pos + r->positions <= (r->dev ? dev_run_positions : run_positions)))
-                    bytes += r->bytes, pos += r->positions, g.push_back(r);
+                                 (r->dev ? seqs + r->n_dev <= dev_run_seqs : pos + r->positions <= run_positions)))
+                    bytes += r->bytes, pos += r->positions, seqs += r->n_dev, g.push_back(r);
                 else
                     rest.push_back(r);
             queue.swap(rest);
@@ -383,12 +379,6 @@ extern "C" int kache_b200_server_new(kache_table* const t, const uint64_t budget
         s->counts.ensure((P / 16) * 8);
         // Staging for the bases of a full-size run of reads of 100 bp or more (positions x 1.5), in both buffers.
         s->stage[0].ensure(P * 3 / 2), s->stage[1].ensure(P * 3 / 2);
-        if(cudaStreamCreateWithFlags(&s->probe, cudaStreamNonBlocking) != cudaSuccess)
-        {
-            delete s;
-            return KACHE_EINTERNAL;
-        }
-        s->probe_buf.ensure(16);
         s->executor = std::thread([s](){ s->execute(); });
         s->worker = std::thread([s](){ s->loop(); });
         *out = s;
@@ -419,8 +409,6 @@ extern "C" void kache_b200_server_free(kache_server* const s) noexcept
         s->executor.join();
     for(auto& kv : s->all)
         delete kv.second;
-    if(s->probe)
-        cudaStreamDestroy(s->probe);
     delete s;
 }
 
@@ -477,31 +465,9 @@ extern "C" int kache_b200_server_submit_dev(kache_server* const s, const uint32_
         auto* r = new Request;
         r->kind = kind, r->op = op, r->x = x, r->init = init, r->out0 = out0, r->out1 = out1, r->out2 = out2;
         r->dev = true, r->d_bases = d_bases, r->d_off = d_off, r->n_dev = n;
-        // The batch's bases bound its positions: read its first and last offsets (a 16-byte copy on the server's
-        // own stream, so a submission never waits for the table's work).
-        uint64_t bases = 0;
-        if(n > 0)
-        {
-            std::lock_guard<std::mutex> lk(s->probe_mu);
-            uint64_t* h = s->probe_buf.as<uint64_t>();
-            if(cudaMemcpyAsync(h, d_off, 8, cudaMemcpyDeviceToHost, s->probe) != cudaSuccess ||
-               cudaMemcpyAsync(h + 1, d_off + n, 8, cudaMemcpyDeviceToHost, s->probe) != cudaSuccess ||
-               cudaStreamSynchronize(s->probe) != cudaSuccess)
-            {
-                delete r;
-                return KACHE_EINTERNAL;
-            }
-            if(h[1] < h[0])
-            {
-                delete r;
-                return KACHE_EINVAL;
-            }
-            bases = h[1] - h[0];
-        }
-        r->positions = bases;
-        // Device bytes of its share of the merged list: offsets, addresses, lengths, per-sequence results and batch
-        // numbers (36 bytes a sequence), and segment entries (8 bytes per 16 positions at most).
-        r->bytes = 36 * n + bases / 2 + 64;
+        // Nothing is read from the device here: a submission never waits for the GPU. Device bytes of its share of
+        // the merged list: offsets, addresses, lengths, per-sequence results and batch numbers, 36 bytes a sequence.
+        r->bytes = 36 * n + 64;
         r->t_submit = clock_type::now();
         {
             std::lock_guard<std::mutex> lk(s->mu);

@@ -603,11 +603,19 @@ def run_config3(args):
         T.run_dev_batches(kache.RUN_LOOKUP, looks)
 
     ms_r = timed_steps(stream, step_runs, args.steps, args.warmup)
-    T.profile(True)
-    step_batched()
-    torch.cuda.synchronize()
-    prof_b = {kind: T.profile_read(i) for i, kind in enumerate(["upsert", "update", "lookup", "reduce", "resize", "other"])}
-    T.profile(False)
+
+    def profiled(f):
+        """Device milliseconds per kernel kind of one run of f (CUDA events around each launch)."""
+        T.profile(True)
+        f()
+        torch.cuda.synchronize()
+        p_ = {kind: T.profile_read(i) for i, kind in enumerate(["upsert", "update", "lookup", "reduce", "resize", "other"])}
+        T.profile(False)
+        return p_
+
+    prof_1 = profiled(step)
+    prof_r = profiled(step_runs)
+    prof_b = profiled(step_batched)
     size, cap = T.size(), T.capacity()
     T.close()
     t_ref, threads = ref_sample(5, n, 0.8, False, [("ref_bench_upsert_oriented", br, (3, 1, 2)), ("lookup", br, (27,))])
@@ -616,10 +624,12 @@ def run_config3(args):
     config_line("k-mers/s upsert_oriented+find (config 3: <27,u8,16> strand map, long reads)", 2 * P1 / (ms * 1e-3), ms,
                 {"workload": f"config 3 at scale {args.scale}: {len(g)} bp genome, {br.n} reads lognormal(10 kb, 0.8) clipped "
                              "1-100 kb at 5x, 5% errors 3:1:1", "positions_per_phase": P1, "keys": size, "capacity": cap},
-                cpu=cpu, extra={"batched_256_reads": {"value": 2 * P1 / (ms_b * 1e-3), "ms_per_step": ms_b, "calls_per_step": 2 * len(pieces),
+                cpu=cpu, extra={"kernel_ms_one_step": {k_: v_[0] for k_, v_ in prof_1.items()},
+                                "batched_256_reads": {"value": 2 * P1 / (ms_b * 1e-3), "ms_per_step": ms_b, "calls_per_step": 2 * len(pieces),
                                                       "kernel_ms_one_step": {k_: v_[0] for k_, v_ in prof_b.items()}},
                                 "run_dev_batches_256_reads": {"value": 2 * P1 / (ms_r * 1e-3), "ms_per_step": ms_r, "calls_per_step": 2,
                                                               "batches_per_call": len(pieces),
+                                                              "kernel_ms_one_step": {k_: v_[0] for k_, v_ in prof_r.items()},
                                                               "vs_one_call_per_batch": ms_b / ms_r}})
 
 

@@ -462,41 +462,35 @@ static __global__ void batches_scatter_kernel(const uint64_t* desc, const unsign
     }
 }
 
-// Per-batch present positions of a lookup of several batches: each thread counts the found flags equal to 1 over
-// chunks of 64 merged positions, read from the batch's own array (desc word 4) and flushed at batch changes.
-// pos_base[b] is batch b's first merged position (non-decreasing in b); P is the merged positions.
-static __global__ void batches_hits_kernel(const uint64_t* desc, const uint64_t* pos_base, const uint64_t count,
-                                           const uint64_t P, unsigned long long* per_batch)
+// Per-sequence positions found (found flag 1) of a lookup of several batches, read back from each batch's found array
+// (desc word 4): a warp per sequence, 4-byte words where aligned, bytes equal to 1 counted by a zero-byte test of the
+// word XOR 0x01010101.
+static __global__ void batches_hits_kernel(const uint64_t* desc, const uint32_t* batch_of, const uint64_t* pos_off,
+                                           const uint64_t* pos_base, const uint64_t N, unsigned long long* per_seq)
 {
-    const uint64_t chunks = (P + 63) / 64, stride = uint64_t(gridDim.x) * blockDim.x;
-    for(uint64_t c = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; c < chunks; c += stride)
+    const uint32_t lane = threadIdx.x & 31;
+    const uint64_t warps = uint64_t(gridDim.x) * (blockDim.x / 32);
+    for(uint64_t q = uint64_t(blockIdx.x) * (blockDim.x / 32) + (threadIdx.x >> 5); q < N; q += warps)
     {
-        const uint64_t p0 = c * 64, p1 = min(P, p0 + 64);
-        uint64_t lo = 0, hi = count;    // The first batch starting past p0; the one before it holds p0.
-        while(lo < hi)
-        {
-            const uint64_t mid = (lo + hi) / 2;
-            if(pos_base[mid] <= p0)
-                lo = mid + 1;
-            else
-                hi = mid;
-        }
-        uint64_t b = lo - 1;
-        uint64_t end = b + 1 < count ? pos_base[b + 1] : P;
-        unsigned long long acc = 0;
-        for(uint64_t p = p0; p < p1; ++p)
-        {
-            while(p >= end)
-            {
-                if(acc)
-                    atomicAdd(per_batch + b, acc), acc = 0;
-                ++b;
-                end = b + 1 < count ? pos_base[b + 1] : P;
-            }
-            acc += reinterpret_cast<const uint8_t*>(desc[8 * b + 4])[p - pos_base[b]] == 1;
-        }
-        if(acc)
-            atomicAdd(per_batch + b, acc);
+        const uint32_t b = batch_of[q];
+        const uint8_t* f = reinterpret_cast<const uint8_t*>(desc[8 * uint64_t(b) + 4]) + (pos_off[q] - pos_base[b]);
+        const uint64_t m = pos_off[q + 1] - pos_off[q];
+        const uint64_t lead = (4 - (reinterpret_cast<uintptr_t>(f) & 3)) & 3, head = m < lead ? m : lead;
+        const uint64_t nw = (m - head) / 4, tail = head + 4 * nw;
+        const uint32_t* w = reinterpret_cast<const uint32_t*>(f + head);
+        unsigned long long c = 0;
+        if(lane < head)
+            c += f[lane] == 1;
+#pragma unroll 4
+        for(uint64_t i = lane; i < nw; i += 32)
+            c += __popc(zero_bytes(w[i] ^ 0x01010101u));
+        if(tail + lane < m)
+            c += f[tail + lane] == 1;
+#pragma unroll
+        for(int o = 16; o > 0; o >>= 1)
+            c += __shfl_xor_sync(0xFFFFFFFFu, c, o);
+        if(lane == 0)
+            per_seq[q] = c;
     }
 }
 

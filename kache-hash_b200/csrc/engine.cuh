@@ -1452,8 +1452,7 @@ public:
         bi.b.seq_addr = addr;
         dout_.ensure(N * 8 + 8);
         auto* per_seq = dout_.as<unsigned long long>();
-        if(kind != KACHE_B200_RUN_LOOKUP)
-            check(cudaMemsetAsync(per_seq, 0, N * 8, stream_), "memset");
+        check(cudaMemsetAsync(per_seq, 0, N * 8, stream_), "memset");
         if(kind == KACHE_B200_RUN_UPSERT)
             run_upsert(user, bi, op_fn(op, x, y), per_seq);
         else if(kind == KACHE_B200_RUN_UPSERT_ORIENTED)
@@ -1481,14 +1480,12 @@ public:
             launch(K_OTHER, [&](){ batches_pos_kernel<<<static_cast<unsigned>((count + 255) / 256), 256, 0, stream_>>>(desc, count, bi.b.pos_off, pos_base); });
             Lookup_Batches_Visitor<set_, VT> vis{{T_, bi.b.pos_off, nullptr, nullptr, nullptr, 0}, batch_of, desc, pos_base};
             stream_launch(K_LOOKUP, bi, 0, bi.b.nsegs, vis, true);
+            launch(K_OTHER, [&](){ batches_hits_kernel<<<grid_for(N, 8), 256, 0, stream_>>>(desc, batch_of, bi.b.pos_off, pos_base, N, per_seq); });
         }
-        // Per-batch results: the per-sequence counters summed per batch (keys inserted, k-mers present, counts), or
-        // a lookup's found flags equal to 1 counted per batch.
+        // Per-batch results: the per-sequence counters (keys inserted, k-mers present, positions found, counts)
+        // summed per batch.
         check(cudaMemsetAsync(res, 0, count * 8, stream_), "memset");
-        if(kind != KACHE_B200_RUN_LOOKUP)
-            launch(K_OTHER, [&](){ batches_sum_kernel<<<grid_for((N + 31) / 32 / 64 + 1, 8), 256, 0, stream_>>>(per_seq, batch_of, N, res); });
-        else if(bi.total_pos > 0)
-            launch(K_OTHER, [&](){ batches_hits_kernel<<<grid_for((bi.total_pos + 63) / 64 / 32 + 1, 8), 256, 0, stream_>>>(desc, pos_base, count, bi.total_pos, res); });
+        launch(K_OTHER, [&](){ batches_sum_kernel<<<grid_for((N + 31) / 32 / 64 + 1, 8), 256, 0, stream_>>>(per_seq, batch_of, N, res); });
         auto* hr = pin_multi_.as<uint64_t>();
         check(cudaMemcpyAsync(hr, res, count * 8, cudaMemcpyDeviceToHost, stream_), "D2H results");
         sync();

@@ -80,13 +80,17 @@ def test_upsert_lookup_count_update(vb):
     ko, vo = O.dump()
     assert np.array_equal(kg, ko) and np.array_equal(vg, vo)
 
-    # Lookups: each batch's own arrays, as a lookup of that batch alone.
+    # Lookups: each batch's own arrays, as a lookup of that batch alone. The found flags lie in one buffer at offsets
+    # of every residue mod 4, so the per-batch count of found flags reads unaligned heads and tails.
     dev = torch.device("cuda", 0)
     outs = []
+    fbuf = torch.full((sum(max(1, _positions(b)) + 1 for b in host) + 1,), 7, dtype=torch.uint8, device=dev)
+    at = 1
     for b in host:
         P = max(1, _positions(b))
-        outs.append((torch.full((P,), 7, dtype=torch.uint8, device=dev), torch.zeros(P * vb, dtype=torch.uint8, device=dev),
+        outs.append((fbuf[at:at + P], torch.zeros(P * vb, dtype=torch.uint8, device=dev),
                      torch.full((P,), 7, dtype=torch.uint8, device=dev)))
+        at += P + 1
     hits = G.run_dev_batches(kache.RUN_LOOKUP, [(b.data_ptr(), o.data_ptr(), n, f.data_ptr(), v.data_ptr(), w.data_ptr())
                                                  for (b, o, n), (f, v, w) in zip(devb, outs)])
     dt = {8: np.uint64, 4: np.uint32, 1: np.uint8}[vb]

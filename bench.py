@@ -604,6 +604,30 @@ def run_config3(args):
 
     ms_r = timed_steps(stream, step_runs, args.steps, args.warmup)
 
+    # The lookups of the same 256-read batches (on the table step_runs left): one staged call per batch; the batch
+    # shapes prepared once and the 71 launches captured in a CUDA graph, replayed; one batched call.
+    def look_calls():
+        for i_, (b_, o_, n_) in enumerate(pieces):
+            at = int(starts[i_])
+            T.lookup_dev(b_.data_ptr(), o_.data_ptr(), n_, found[at:].data_ptr(), vals[at:].data_ptr(), fwd[at:].data_ptr())
+
+    ms_lc = timed_steps(stream, look_calls, args.steps, args.warmup)
+    ms_lb = timed_steps(stream, lambda: T.run_dev_batches(kache.RUN_LOOKUP, looks), args.steps, args.warmup)
+    preps = [T.prepare_dev(o_.data_ptr(), n_) for _, o_, n_ in pieces]
+    cap_stream = torch.cuda.Stream()
+    T.set_stream(cap_stream.cuda_stream)
+    torch.cuda.synchronize()
+    graph = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(graph, stream=cap_stream):
+        for i_, ((b_, o_, n_), p_) in enumerate(zip(pieces, preps)):
+            at = int(starts[i_])
+            T.lookup_prepared(p_, b_.data_ptr(), found[at:].data_ptr(), vals[at:].data_ptr(), fwd[at:].data_ptr())
+    ms_lg = timed_steps(stream, graph.replay, args.steps, args.warmup)     # replay() runs on the current stream
+    del graph
+    T.set_stream(stream.cuda_stream)
+    for p_ in preps:
+        T.prepared_free(p_)
+
     def profiled(f):
         """Device milliseconds per kernel kind of one run of f (CUDA events around each launch)."""
         T.profile(True)
@@ -630,7 +654,11 @@ def run_config3(args):
                                 "run_dev_batches_256_reads": {"value": 2 * P1 / (ms_r * 1e-3), "ms_per_step": ms_r, "calls_per_step": 2,
                                                               "batches_per_call": len(pieces),
                                                               "kernel_ms_one_step": {k_: v_[0] for k_, v_ in prof_r.items()},
-                                                              "vs_one_call_per_batch": ms_b / ms_r}})
+                                                              "vs_one_call_per_batch": ms_b / ms_r},
+                                "lookups_256_reads": {"positions": P1, "batches": len(pieces), "per_call_ms": ms_lc,
+                                                      "cuda_graph_ms": ms_lg, "run_dev_batches_ms": ms_lb,
+                                                      "cuda_graph": "kache_b200_prepare_dev once per batch shape, the "
+                                                                    "kache_b200_lookup_prepared launches captured in one graph"}})
 
 
 def run_config4(args):

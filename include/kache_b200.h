@@ -74,6 +74,21 @@ typedef struct kache_dev_batch {
 #define KACHE_B200_RUN_COUNT           4u
 int kache_b200_run_dev_batches(kache_table* t, uint32_t user, uint32_t kind, uint32_t op, uint64_t x, uint64_t y, kache_dev_batch* batches, size_t count) KACHE_NOEXCEPT;
 
+/* Lookups that can be captured in a CUDA graph (no counterpart in the reference): a batch shape -- n sequences with
+ * the device offsets d_off[0..n] -- is staged once by kache_b200_prepare_dev (which synchronises); then
+ * kache_b200_lookup_prepared looks up any batch with those offsets (the same lengths, any bases) as ONE kernel launch
+ * on the table's stream: no staging, no allocation, no synchronisation, so a caller can capture a run of them, e.g.
+ * one per batch of a batch-size class, in a CUDA graph and replay it. Outputs are device arrays laid out as
+ * kache_lookup's; the call returns before the lookup has run (synchronise with the table's stream, or the graph, to
+ * read them). A launch captured in a graph takes the table's device arrays as they were at capture: replay it only
+ * while kache_b200_table_epoch returns the value it returned at capture (upserts that grow the table, clears and
+ * overflow growth move the arrays); otherwise capture again. A handle belongs to the table that made it. */
+typedef struct kache_prepared kache_prepared;
+int kache_b200_prepare_dev(kache_table* t, const uint64_t* d_off, uint64_t n, kache_prepared** out) KACHE_NOEXCEPT;
+void kache_b200_prepared_free(kache_prepared* p) KACHE_NOEXCEPT;
+int kache_b200_lookup_prepared(kache_table* t, const kache_prepared* p, const uint8_t* d_bases, uint8_t* d_found, void* d_values, uint8_t* d_fwd) KACHE_NOEXCEPT;
+int kache_b200_table_epoch(kache_table* t, uint64_t* epoch) KACHE_NOEXCEPT;
+
 /* kache_b200_count_dev for callers that cannot allocate device memory: no counterpart in the reference.
  *
  * Callers running inside their own memory pool, inside a CUDA graph capture, or in a process that budgets every byte

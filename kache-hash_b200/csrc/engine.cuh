@@ -55,6 +55,10 @@ struct kache_table
     virtual void lookup_dev(const uint8_t* b, const uint64_t* off, uint64_t n, uint8_t* found, void* values, uint8_t* fwd) = 0;
     virtual void count_dev(const uint8_t* b, const uint64_t* off, uint64_t n, uint64_t* counts) = 0;
     virtual void run_dev_batches(uint32_t user, uint32_t kind, uint32_t op, uint64_t x, uint64_t y, kache_dev_batch* bs, size_t count) = 0;
+    // A batch shape staged once (kache_b200_prepare_dev), and lookups of batches of that shape that only launch.
+    virtual kache_prepared* prepare_dev(const uint64_t* off, uint64_t n) = 0;
+    virtual void lookup_prepared(const kache_prepared& p, const uint8_t* b, uint8_t* found, void* values, uint8_t* fwd) = 0;
+    virtual uint64_t epoch() = 0;
     virtual bool get(const char* kmer, uint64_t& value) = 0;
     virtual uint64_t size() const = 0;
     virtual uint64_t capacity() const = 0;
@@ -341,6 +345,21 @@ private:
     }
 };
 
+}
+
+// A batch shape staged once: its offsets, each sequence's first position, and the list of its 512-position segments,
+// all in device memory owned here, for lookups that launch without staging (kache_b200_lookup_prepared).
+struct kache_prepared
+{
+    const kache_table* t = nullptr;     // The table that staged it.
+    kache_b200::Dev_Buf off, pos_off, segs;
+    uint64_t n = 0, nsegs = 0, total_pos = 0;
+    uint32_t seg_len = 0;
+};
+
+namespace kache_b200
+{
+
 // ---- The engine --------------------------------------------------------------------------------------------------
 
 enum Kind : uint32_t { K_UPSERT = 0, K_UPDATE = 1, K_LOOKUP = 2, K_REDUCE = 3, K_RESIZE = 4, K_OTHER = 5, K_KINDS = 6 };
@@ -354,6 +373,8 @@ class Engine final : public kache_table
 
     cudaStream_t own_ = nullptr, stream_ = nullptr;
     int sm_count_ = 148;
+    Dev_Table epoch_T_{};   // The arrays epoch() last saw, and its count of changes.
+    uint64_t epoch_ = 0;
 
     // The table.
     Dev_Buf cs_, spill_, slots_, ov_, ctr_;
@@ -1386,6 +1407,57 @@ public:
         const auto bi = stage_dev(b, off, n, false);
         run_lookup(bi, found, set_ ? nullptr : static_cast<VT*>(values), fwd);
         sync();
+    }
+
+    // Stages a batch shape once: the lookup's segment list and each sequence's first position, copied into the
+    // handle, so that lookups of batches with these offsets need neither staging nor a sync.
+    kache_prepared* prepare_dev(const uint64_t* off, const uint64_t n) override
+    {
+        std::lock_guard<std::mutex> g(work);
+        const auto bi = stage_dev(nullptr, off, n, false);
+        auto* p = new kache_prepared;
+        try
+        {
+            p->t = this, p->n = n, p->nsegs = bi.b.nsegs, p->total_pos = bi.total_pos, p->seg_len = bi.b.seg_len;
+            p->off.ensure((n + 1) * 8), p->pos_off.ensure((n + 1) * 8), p->segs.ensure(bi.b.nsegs * 8 + 8);
+            if(n > 0)
+            {
+                check(cudaMemcpyAsync(p->off.p, off, (n + 1) * 8, cudaMemcpyDeviceToDevice, stream_), "copy");
+                check(cudaMemcpyAsync(p->pos_off.p, bi.b.pos_off, (n + 1) * 8, cudaMemcpyDeviceToDevice, stream_), "copy");
+            }
+            if(bi.b.nsegs)
+                check(cudaMemcpyAsync(p->segs.p, bi.b.segs, bi.b.nsegs * 8, cudaMemcpyDeviceToDevice, stream_), "copy");
+            sync();
+        }
+        catch(...)
+        {
+            delete p;
+            throw;
+        }
+        return p;
+    }
+
+    // A lookup of a batch of the prepared shape: one launch on the table's stream, no staging, no allocation, no
+    // sync, so it can be captured in a CUDA graph. The launch takes the table's arrays as they are now.
+    void lookup_prepared(const kache_prepared& p, const uint8_t* b, uint8_t* found, void* values, uint8_t* fwd) override
+    {
+        std::lock_guard<std::mutex> g(work);
+        Batch_Info bi;
+        bi.b = Dev_Batch{b, p.off.as<uint64_t>(), p.segs.as<uint64_t>(), p.pos_off.as<uint64_t>(), p.n, p.nsegs, p.seg_len};
+        bi.total_pos = p.total_pos;
+        run_lookup(bi, found, set_ ? nullptr : static_cast<VT*>(values), fwd);
+    }
+
+    // A number that stays the same while the table's device arrays do (a graph captured with a prepared lookup stays
+    // valid), and changes when a call moved them (a rebuild, a clear, a larger overflow table).
+    uint64_t epoch() override
+    {
+        std::lock_guard<std::mutex> g(work);
+        const Dev_Table& a = epoch_T_;
+        if(a.cs != T_.cs || a.spill != T_.spill || a.slots != T_.slots || a.cap != T_.cap || a.ov != T_.ov ||
+           a.ov_mask != T_.ov_mask || a.ov_probe != T_.ov_probe || a.ov_count != T_.ov_count || a.err != T_.err)
+            epoch_T_ = T_, ++epoch_;
+        return epoch_;
     }
 
     void count_dev(const uint8_t* b, const uint64_t* off, uint64_t n, uint64_t* counts) override

@@ -401,6 +401,38 @@ int kache_b200_run_dev_batches(kache_table* const t, const uint32_t user, const 
     return guard([&](){ return t->run_dev_batches(user, kind, op, x, y, batches, count), KACHE_OK; });
 }
 
+int kache_b200_prepare_dev(kache_table* const t, const uint64_t* const d_off, const uint64_t n, kache_prepared** const out) noexcept
+{
+    if(t == nullptr || out == nullptr || (n > 0 && d_off == nullptr))
+        return KACHE_EINVAL;
+    *out = nullptr;
+    return guard([&](){ return *out = t->prepare_dev(d_off, n), KACHE_OK; });
+}
+
+void kache_b200_prepared_free(kache_prepared* const p) noexcept
+{
+    delete p;
+}
+
+int kache_b200_lookup_prepared(kache_table* const t, const kache_prepared* const p, const uint8_t* const d_bases, uint8_t* const d_found,
+                               void* const d_values, uint8_t* const d_fwd) noexcept
+{
+    if(t == nullptr || p == nullptr || p->t != t)
+        return KACHE_EINVAL;
+    if(p->total_pos > 0 && (d_bases == nullptr || d_found == nullptr))
+        return KACHE_EINVAL;
+    if(t->value_bytes == 0 && d_values != nullptr)
+        return KACHE_EINVAL;
+    return guard([&](){ return t->lookup_prepared(*p, d_bases, d_found, d_values, d_fwd), KACHE_OK; });
+}
+
+int kache_b200_table_epoch(kache_table* const t, uint64_t* const epoch) noexcept
+{
+    if(t == nullptr || epoch == nullptr)
+        return KACHE_EINVAL;
+    return guard([&](){ return *epoch = t->epoch(), KACHE_OK; });
+}
+
 int kache_b200_describe(kache_table* const t, const char* const* const seqs, const size_t* const lens, const size_t n, uint64_t* const key, uint64_t* const h, uint8_t* const cs, uint8_t* const fwd, uint8_t* const valid_out) noexcept
 {
     if(t == nullptr || !valid(seqs, lens, n) || !key || !h || !cs || !fwd || !valid_out)

@@ -94,6 +94,10 @@ def lib():
             "kache_b200_lookup_dev": (ctypes.c_int, [_vp, _vp, _vp, ctypes.c_uint64, _vp, _vp, _vp]),
             "kache_b200_count_dev": (ctypes.c_int, [_vp, _vp, _vp, ctypes.c_uint64, _vp]),
             "kache_b200_run_dev_batches": (ctypes.c_int, [_vp, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint64, ctypes.c_uint64, ctypes.POINTER(DevBatch), ctypes.c_size_t]),
+            "kache_b200_prepare_dev": (ctypes.c_int, [_vp, _vp, ctypes.c_uint64, ctypes.POINTER(_vp)]),
+            "kache_b200_prepared_free": (None, [_vp]),
+            "kache_b200_lookup_prepared": (ctypes.c_int, [_vp, _vp, _vp, _vp, _vp, _vp]),
+            "kache_b200_table_epoch": (ctypes.c_int, [_vp, _u64p]),
             "kache_b200_describe": (ctypes.c_int, [_vp, _vp, _vp, ctypes.c_size_t, _vp, _vp, _vp, _vp, _vp]),
             "kache_b200_histogram": (ctypes.c_int, [_vp, ctypes.c_uint64, _vp]),
             "kache_b200_clear": (ctypes.c_int, [_vp]),
@@ -321,6 +325,26 @@ class Table:
 
     def lookup_dev(self, d_bases, d_off, n, d_found, d_values=None, d_fwd=None):
         _check(lib().kache_b200_lookup_dev(self.h, d_bases, d_off, n, d_found, d_values, d_fwd), "lookup_dev")
+
+    def prepare_dev(self, d_off, n):
+        """Stages the batch shape of the device offsets d_off[0..n] once (kache_b200_prepare_dev); returns the handle
+        for lookup_prepared. Free it with prepared_free."""
+        p = _vp()
+        _check(lib().kache_b200_prepare_dev(self.h, d_off, n, ctypes.byref(p)), "prepare_dev")
+        return p
+
+    @staticmethod
+    def prepared_free(p):
+        lib().kache_b200_prepared_free(p)
+
+    def lookup_prepared(self, p, d_bases, d_found, d_values=None, d_fwd=None):
+        """One lookup launch of a batch of the prepared shape on the table's stream; returns before it has run."""
+        _check(lib().kache_b200_lookup_prepared(self.h, p, d_bases, d_found, d_values, d_fwd), "lookup_prepared")
+
+    def epoch(self):
+        e = ctypes.c_uint64()
+        _check(lib().kache_b200_table_epoch(self.h, ctypes.byref(e)), "table_epoch")
+        return e.value
 
     def count_dev(self, d_bases, d_off, n, d_counts):
         _check(lib().kache_b200_count_dev(self.h, d_bases, d_off, n, d_counts), "count_dev")

@@ -87,6 +87,9 @@ typedef struct kache_prepared kache_prepared;
 int kache_b200_prepare_dev(kache_table* t, const uint64_t* d_off, uint64_t n, kache_prepared** out) KACHE_NOEXCEPT;
 void kache_b200_prepared_free(kache_prepared* p) KACHE_NOEXCEPT;
 int kache_b200_lookup_prepared(kache_table* t, const kache_prepared* p, const uint8_t* d_bases, uint8_t* d_found, void* d_values, uint8_t* d_fwd) KACHE_NOEXCEPT;
+/* Per-sequence counts of present k-mers (kache_count's) of a batch of the prepared shape, into the device array
+ * d_counts[0..n): a memset and one launch on the table's stream, capturable as kache_b200_lookup_prepared is. */
+int kache_b200_count_prepared(kache_table* t, const kache_prepared* p, const uint8_t* d_bases, uint64_t* d_counts) KACHE_NOEXCEPT;
 int kache_b200_table_epoch(kache_table* t, uint64_t* epoch) KACHE_NOEXCEPT;
 
 /* kache_b200_count_dev for callers that cannot allocate device memory: no counterpart in the reference.

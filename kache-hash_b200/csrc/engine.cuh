@@ -58,6 +58,7 @@ struct kache_table
     // A batch shape staged once (kache_b200_prepare_dev), and lookups of batches of that shape that only launch.
     virtual kache_prepared* prepare_dev(const uint64_t* off, uint64_t n) = 0;
     virtual void lookup_prepared(const kache_prepared& p, const uint8_t* b, uint8_t* found, void* values, uint8_t* fwd) = 0;
+    virtual void count_prepared(const kache_prepared& p, const uint8_t* b, uint64_t* counts) = 0;
     virtual uint64_t epoch() = 0;
     virtual bool get(const char* kmer, uint64_t& value) = 0;
     virtual uint64_t size() const = 0;
@@ -1446,6 +1447,20 @@ public:
         bi.b = Dev_Batch{b, p.off.as<uint64_t>(), p.segs.as<uint64_t>(), p.pos_off.as<uint64_t>(), p.n, p.nsegs, p.seg_len};
         bi.total_pos = p.total_pos;
         run_lookup(bi, found, set_ ? nullptr : static_cast<VT*>(values), fwd);
+    }
+
+    // Per-sequence counts of present k-mers of a batch of the prepared shape: a memset and one launch of the warp
+    // kernel (one atomic per segment), capturable as lookup_prepared is.
+    void count_prepared(const kache_prepared& p, const uint8_t* b, uint64_t* counts) override
+    {
+        std::lock_guard<std::mutex> g(work);
+        Batch_Info bi;
+        bi.b = Dev_Batch{b, p.off.as<uint64_t>(), p.segs.as<uint64_t>(), p.pos_off.as<uint64_t>(), p.n, p.nsegs, p.seg_len};
+        bi.total_pos = p.total_pos;
+        auto* out = reinterpret_cast<unsigned long long*>(counts);
+        if(p.n)
+            check(cudaMemsetAsync(out, 0, p.n * 8, stream_), "memset");
+        stream_launch(K_REDUCE, bi, 0, bi.b.nsegs, Seq_Reduce_Visitor<set_, VT, 0>{T_, out, VT(0), VT(0), 0, 0}, true);
     }
 
     // A number that stays the same while the table's device arrays do (a graph captured with a prepared lookup stays

@@ -426,6 +426,15 @@ int kache_b200_lookup_prepared(kache_table* const t, const kache_prepared* const
     return guard([&](){ return t->lookup_prepared(*p, d_bases, d_found, d_values, d_fwd), KACHE_OK; });
 }
 
+int kache_b200_count_prepared(kache_table* const t, const kache_prepared* const p, const uint8_t* const d_bases, uint64_t* const d_counts) noexcept
+{
+    if(t == nullptr || p == nullptr || p->t != t)
+        return KACHE_EINVAL;
+    if(p->n > 0 && (d_bases == nullptr || d_counts == nullptr))
+        return KACHE_EINVAL;
+    return guard([&](){ return t->count_prepared(*p, d_bases, d_counts), KACHE_OK; });
+}
+
 int kache_b200_table_epoch(kache_table* const t, uint64_t* const epoch) noexcept
 {
     if(t == nullptr || epoch == nullptr)

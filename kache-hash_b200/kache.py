@@ -98,6 +98,7 @@ def lib():
             "kache_b200_prepared_free": (None, [_vp]),
             "kache_b200_lookup_prepared": (ctypes.c_int, [_vp, _vp, _vp, _vp, _vp, _vp]),
             "kache_b200_table_epoch": (ctypes.c_int, [_vp, _u64p]),
+            "kache_b200_count_prepared": (ctypes.c_int, [_vp, _vp, _vp, _vp]),
             "kache_b200_describe": (ctypes.c_int, [_vp, _vp, _vp, ctypes.c_size_t, _vp, _vp, _vp, _vp, _vp]),
             "kache_b200_histogram": (ctypes.c_int, [_vp, ctypes.c_uint64, _vp]),
             "kache_b200_clear": (ctypes.c_int, [_vp]),
@@ -340,6 +341,10 @@ class Table:
     def lookup_prepared(self, p, d_bases, d_found, d_values=None, d_fwd=None):
         """One lookup launch of a batch of the prepared shape on the table's stream; returns before it has run."""
         _check(lib().kache_b200_lookup_prepared(self.h, p, d_bases, d_found, d_values, d_fwd), "lookup_prepared")
+
+    def count_prepared(self, p, d_bases, d_counts):
+        """Per-sequence counts of a batch of the prepared shape into d_counts, one launch; returns before it has run."""
+        _check(lib().kache_b200_count_prepared(self.h, p, d_bases, d_counts), "count_prepared")
 
     def epoch(self):
         e = ctypes.c_uint64()

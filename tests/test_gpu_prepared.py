@@ -1,9 +1,10 @@
 """Lookups of prepared batch shapes (kache_b200_prepare_dev, kache_b200_lookup_prepared) through the C interface.
 
-Each prepared lookup equals the staged lookup of the same batch (kache_b200_lookup_dev) bit for bit, for fixed-length,
-ragged, odd (empty, short, non-ACGT, lowercase) and empty batches. A run of them captured in a CUDA graph and replayed
-gives the same outputs, and again after the batches' bases change in place (the same lengths, other k-mers). The
-table's epoch holds while lookups run and changes once an upsert grows the table.
+Each prepared lookup equals the staged lookup of the same batch (kache_b200_lookup_dev) bit for bit, and each prepared
+count the staged count (kache_b200_count_dev), for fixed-length, ragged, odd (empty, short, non-ACGT, lowercase) and
+empty batches. A run of them captured in a CUDA graph and replayed gives the same outputs, and again after the
+batches' bases change in place (the same lengths, other k-mers). The table's epoch holds while queries run and changes
+once an upsert grows the table.
 """
 import numpy as np
 import pytest
@@ -50,6 +51,27 @@ def _staged(T, db, dev):
     return out
 
 
+def _staged_counts(T, db, dev):
+    import torch
+    out = []
+    for bases, off, n, _ in db:
+        c = torch.full((max(n, 1),), 99, dtype=torch.int64, device=dev)
+        T.count_dev(bases.data_ptr(), off.data_ptr(), n, c.data_ptr())
+        torch.cuda.synchronize()
+        out.append(c.cpu().numpy().view(np.uint64)[:n])
+    return out
+
+
+def _counts(db, dev):
+    import torch
+    return [torch.full((max(n, 1),), 99, dtype=torch.int64, device=dev) for _, _, n, _ in db]
+
+
+def _same_counts(cs, want, db):
+    for c, w, (_, _, n, _) in zip(cs, want, db):
+        assert np.array_equal(c.cpu().numpy().view(np.uint64)[:n], w)
+
+
 def _same(outs, want, db):
     for (f, v, w), (wf, wv, ww), (_, _, _, P) in zip(outs, want, db):
         assert np.array_equal(f.cpu().numpy()[:P], wf)
@@ -66,31 +88,38 @@ def test_prepared_lookups_and_graph_replay():
     T.upsert(u, Batch(*synth.reads_fixed(g, 4000, 150, seed=84)), kache.ADD_WRAP, 1, 1)
     db = [_on_device(b, dev) for b in _batches(g)]
     want = _staged(T, db, dev)
+    want_c = _staged_counts(T, db, dev)
     assert any(int((f == 1).sum()) > 0 for f, _, _ in want)
     preps = [T.prepare_dev(off.data_ptr(), n) for _, off, n, _ in db]
 
     # One launch per batch, no staging.
     outs = [_outputs(P, dev) for _, _, _, P in db]
-    for (bases, _, _, _), p, (f, v, w) in zip(db, preps, outs):
+    cs = _counts(db, dev)
+    for (bases, _, _, _), p, (f, v, w), c in zip(db, preps, outs, cs):
         T.lookup_prepared(p, bases.data_ptr(), f.data_ptr(), v.data_ptr(), w.data_ptr())
+        T.count_prepared(p, bases.data_ptr(), c.data_ptr())
     torch.cuda.synchronize()
     _same(outs, want, db)
+    _same_counts(cs, want_c, db)
 
     # The same launches captured in a CUDA graph on the table's stream, then replayed.
     e0 = T.epoch()
     outs = [_outputs(P, dev) for _, _, _, P in db]
+    cs = _counts(db, dev)
     s = torch.cuda.Stream()
     T.set_stream(s.cuda_stream)
     torch.cuda.synchronize()
     graph = torch.cuda.CUDAGraph()
     with torch.cuda.graph(graph, stream=s):
-        for (bases, _, _, _), p, (f, v, w) in zip(db, preps, outs):
+        for (bases, _, _, _), p, (f, v, w), c in zip(db, preps, outs, cs):
             T.lookup_prepared(p, bases.data_ptr(), f.data_ptr(), v.data_ptr(), w.data_ptr())
+            T.count_prepared(p, bases.data_ptr(), c.data_ptr())
     torch.cuda.synchronize()
     assert all(int((f.cpu() == 7).sum()) == f.numel() for f, _, _ in outs)     # captured, not run
     graph.replay()
     torch.cuda.synchronize()
     _same(outs, want, db)
+    _same_counts(cs, want_c, db)
 
     # Other bases of the same lengths (A->C->G->T->A, either case), written in place: the replay looks them up.
     lut = torch.arange(256, dtype=torch.uint8, device=dev)
@@ -105,6 +134,7 @@ def test_prepared_lookups_and_graph_replay():
     want2 = _staged(T, db, dev)
     assert want2[0][0].tolist() != want[0][0].tolist()
     _same(outs, want2, db)
+    _same_counts(cs, _staged_counts(T, db, dev), db)
     assert T.epoch() == e0
 
     # An upsert that grows the table moves its arrays: the epoch says so.
@@ -132,6 +162,10 @@ def test_prepared_validation():
         B.lookup_prepared(pb, bases.data_ptr(), f.data_ptr(), v.data_ptr())     # a set has no values
     with pytest.raises(kache.KacheError):
         A.lookup_prepared(pa, bases.data_ptr(), None)                           # no found array
+    with pytest.raises(kache.KacheError):
+        B.count_prepared(pa, bases.data_ptr(), f.data_ptr())                    # another table's handle
+    with pytest.raises(kache.KacheError):
+        A.count_prepared(pa, bases.data_ptr(), None)                            # no counts array
     A.lookup_prepared(pa, bases.data_ptr(), f.data_ptr(), v.data_ptr(), w.data_ptr())
     B.lookup_prepared(pb, bases.data_ptr(), f.data_ptr())
     torch.cuda.synchronize()

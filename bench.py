@@ -530,14 +530,22 @@ def run_config2(args):
     ms = timed_steps(stream, step, args.steps, args.warmup)
     size, cap = T.size(), T.capacity()
     T.close()
-    # End to end through the counter's C interface with page-locked host batches.
+    # End to end through the counter's C interface with page-locked host batches: a first pass on the new counter
+    # (its staging buffers allocated as it goes), the counter's table emptied (kache_b200_clear keeps them), then
+    # the timed pass.
     pi, pr = pinned_copy(bi), pinned_copy(br)
     C = kache.Counter(n, 16, 0.9)
-    t0 = time.perf_counter()
-    C.prime_batch(pi)
-    C.count_batch(pr)
-    C.histogram(10000)
-    e2e_ms = 1000 * (time.perf_counter() - t0)
+
+    def e2e_pass():
+        t0 = time.perf_counter()
+        C.prime_batch(pi)
+        C.count_batch(pr)
+        C.histogram(10000)
+        return 1000 * (time.perf_counter() - t0)
+
+    first_ms = e2e_pass()
+    kache._check(kache.lib().kache_b200_clear(kache.lib().kache_counter_table(C.h)), "kache_b200_clear")
+    e2e_ms = e2e_pass()
     C.close()
     # The reference on a twentieth of the reads (after priming with the whole genome, untimed for the sample rate).
     rs = br.slice(0, br.n // 20)
@@ -550,6 +558,7 @@ def run_config2(args):
                  "count_positions": positions(br.off), "keys": size, "capacity": cap, "found": hist["found"],
                  "histogram_sum": int(sum(hist["h"]))},
                 e2e={"value": P / (e2e_ms * 1e-3), "unit": "k-mers/s", "ms_per_step": e2e_ms, "host_buffers": "page-locked",
+                     "first_pass_ms": first_ms,
                      "calls": "kache_counter_prime_batch, kache_counter_count_batch, kache_counter_histogram"},
                 cpu=cpu)
 

@@ -82,7 +82,8 @@ int kache_b200_run_dev_batches(kache_table* t, uint32_t user, uint32_t kind, uin
  * kache_lookup's; the call returns before the lookup has run (synchronise with the table's stream, or the graph, to
  * read them). A launch captured in a graph takes the table's device arrays as they were at capture: replay it only
  * while kache_b200_table_epoch returns the value it returned at capture (upserts that grow the table, clears and
- * overflow growth move the arrays); otherwise capture again. A handle belongs to the table that made it. */
+ * overflow growth move the arrays); otherwise capture again. A handle belongs to the table that made it; free it
+ * (kache_b200_prepared_free) only once no launch or graph that uses it remains to run. */
 typedef struct kache_prepared kache_prepared;
 int kache_b200_prepare_dev(kache_table* t, const uint64_t* d_off, uint64_t n, kache_prepared** out) KACHE_NOEXCEPT;
 void kache_b200_prepared_free(kache_prepared* p) KACHE_NOEXCEPT;

@@ -95,15 +95,16 @@ int kache_b200_table_epoch(kache_table* t, uint64_t* epoch) KACHE_NOEXCEPT;
 
 /* kache_b200_count_dev for callers that cannot allocate device memory: no counterpart in the reference.
  *
- * Callers running inside their own memory pool, inside a CUDA graph capture, or in a process that budgets every byte
- * of HBM itself cannot let the library call cudaMalloc on a query. This entry point allocates nothing: its scratch
- * (the batch's segment list) lives in one fixed 8 MiB device array that every GPU which loads the library holds until
- * the process exits. It takes at most KACHE_B200_NOALLOC_MAX_SEGMENTS sequences and as many segments of up to 512
- * k-mer positions; beyond that it returns KACHE_EINVAL (up front when n is over the limit, after the kernels when
- * the segments are). Tables of 31-mers with 22-minimizers only (those of kache_new). Every call shares the array and
- * clears its header first, so calls whose GPU work overlaps (other streams or threads) race: serialise them. The
- * first call on a device looks the array's device address up (cudaGetSymbolAddress); make that first call before
- * any stream capture. The call returns synchronised with the table's stream. */
+ * Callers running inside their own memory pool (whose allocator must not be re-entered) or in a process that budgets
+ * every byte of HBM itself cannot let the library call cudaMalloc on a query. This entry point allocates nothing: its
+ * scratch (the batch's segment list) lives in one fixed 8 MiB device array that every GPU which loads the library
+ * holds until the process exits. It takes at most KACHE_B200_NOALLOC_MAX_SEGMENTS sequences and as many segments of
+ * up to 512 k-mer positions; beyond that it returns KACHE_EINVAL, up front when n is over the limit, else after
+ * listing the segments, in which case nothing is counted and d_counts[0..n) holds zeros. Tables of 31-mers with
+ * 22-minimizers only (those of kache_new). Every call shares the array and clears its header first, so calls whose
+ * GPU work overlaps (other streams or threads) race: serialise them. The first call on a device looks the array's
+ * device address up (cudaGetSymbolAddress); make that first call before any stream capture. The call reads a flag
+ * back from the device and returns synchronised with the table's stream. */
 #define KACHE_B200_NOALLOC_MAX_SEGMENTS 1048544ull
 int kache_b200_count_dev_noalloc(kache_table* t, const uint8_t* d_bases, const uint64_t* d_off, uint64_t n, uint64_t* d_counts) KACHE_NOEXCEPT;
 

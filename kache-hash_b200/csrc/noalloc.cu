@@ -1,9 +1,9 @@
 // Per-sequence counts over a batch already in device memory, for callers that cannot allocate device memory.
 //
 // Some callers cannot call cudaMalloc on the path where they query the table: code running inside a memory pool
-// whose allocator must not be re-entered, a CUDA graph being captured (where a new allocation is not allowed), or an
-// embedding process that budgets every byte of HBM itself. kache_b200_count_dev allocates the scratch it needs
-// (segment lists, scan buffers) on first use and whenever a batch outgrows it. This variant does the same counting
+// whose allocator must not be re-entered, or an embedding process that budgets every byte of HBM itself.
+// kache_b200_count_dev allocates the scratch it needs (segment lists, scan buffers) on first use and whenever a batch
+// outgrows it. This variant does the same counting
 // with its scratch in one fixed array below, which every GPU that loads the library holds until the process exits,
 // and calls no cudaMalloc, cudaFree or allocating library routine.
 //
@@ -53,6 +53,11 @@ __global__ void noalloc_segments_kernel(const uint64_t* off, const uint64_t n, c
     const uint64_t nseg = (p + seg_positions - 1) / seg_positions;
     if(nseg == 0)
         return;
+    if(nseg - 1 > max_seg_index)
+    {
+        atomicOr(s.overflow, 1u);   // Segment indexes take 24 bits of an entry: a longer sequence cannot be listed.
+        return;
+    }
     const uint64_t at = atomicAdd(s.count, static_cast<unsigned long long>(nseg));
     if(at + nseg > noalloc_max_segments)
     {
@@ -64,7 +69,9 @@ __global__ void noalloc_segments_kernel(const uint64_t* off, const uint64_t n, c
 }
 
 // The streaming kernel's segment loop (device_stream.cuh) over the listed segments, with the per-sequence count
-// visitor; the segment count comes from the scratch.
+// visitor; the segment count comes from the scratch. A batch that did not fit (the overflow flag) is not counted at
+// all: a sequence whose claim ran past the end wrote none of the entries it claimed, so entries below the end may
+// still hold an earlier call's segments, whose sequence indexes need not exist in this batch.
 template <int k, int l, bool set_>
 __global__ void __launch_bounds__(32 * stream_warps) noalloc_count_kernel(const Dev_Table T, const uint8_t* bases, const uint64_t* off, const Scratch s, unsigned long long* counts)
 {
@@ -72,6 +79,8 @@ __global__ void __launch_bounds__(32 * stream_warps) noalloc_count_kernel(const 
     __shared__ uint64_t ring_all[stream_warps][64];
     const uint32_t lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     uint64_t* ring = ring_all[wid];
+    if(*s.overflow)
+        return;
     Seq_Reduce_Visitor<set_, uint8_t, 0> vis{T, counts, 0, 0, 0, 0};
     vis.begin();
 

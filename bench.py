@@ -725,23 +725,16 @@ def run_config5(args):
     import kache
     from kache import Batch
     dev = torch.device("cuda", 0)
-    rng = np.random.default_rng(53)
-    glen = int(2_000_000_000 * args.scale)
-    g = synth.genome(glen, seed=51)
+    rng = np.random.default_rng(54)     # arrival times
+    g, primer, reqs = synth.config5(args.scale, args.requests)
+    glen = len(g)
     T = kache.Table(31, 4, glen, 0.8, False)
     u = T.register()
-    ib, io, ni = dev_batch(Batch(*synth.stretches(g, 1_000_000)), dev)
+    ib, io, ni = dev_batch(Batch(*primer), dev)
     T.upsert_dev(u, ib.data_ptr(), io.data_ptr(), ni, kache.KEEP, 0, 0)
     torch.cuda.synchronize()
     primed = T.size()
     del ib, io
-    pool = Batch(*synth.reads_fixed(g, min(4_000_000, max(100_000, glen // 100)), 150, seed=52, sub=0.01, n_rate=0.0005))
-    reqs = []
-    for _ in range(args.requests):
-        kind = rng.choice(3, p=[0.6, 0.3, 0.1])
-        m = int(np.clip(rng.lognormal(np.log(2000), 1.5), 1, min(1_000_000, pool.n)))
-        s = int(rng.integers(0, pool.n - m + 1))
-        reqs.append((int(kind), pool.slice(s, s + m)))
     P = sum(int(b.positions(31).sum()) for _, b in reqs)
 
     def outputs(kind, b):

@@ -54,6 +54,37 @@ RUN_UPSERT, RUN_UPSERT_ORIENTED, RUN_UPDATE, RUN_LOOKUP, RUN_COUNT = range(5)
 
 KEYS_FN = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, _u64p, ctypes.c_void_p, ctypes.c_size_t)
 
+# The reference's C interface (capi/kache_capi.h:111-202): prototypes as ctypes signatures.
+CAPI_SIGS = {
+    "kache_supports": (ctypes.c_int, [ctypes.c_uint32, ctypes.c_uint32]),
+    "kache_default_options": (Options, [ctypes.c_uint32, ctypes.c_uint32]),
+    "kache_new": (ctypes.c_int, [ctypes.POINTER(Options), ctypes.POINTER(_vp)]),
+    "kache_free": (None, [_vp]),
+    "kache_register": (ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_uint32)]),
+    "kache_insert": (ctypes.c_int, [_vp, ctypes.c_uint32, _vp, _vp, ctypes.c_size_t, ctypes.c_uint32, ctypes.c_uint64, _u64p]),
+    "kache_insert_oriented": (ctypes.c_int, [_vp, ctypes.c_uint32, _vp, _vp, ctypes.c_size_t, ctypes.c_uint32, ctypes.c_uint64, ctypes.c_uint64, _u64p]),
+    "kache_update": (ctypes.c_int, [_vp, _vp, _vp, ctypes.c_size_t, ctypes.c_uint32, ctypes.c_uint64, _u64p]),
+    "kache_count": (ctypes.c_int, [_vp, _vp, _vp, ctypes.c_size_t, _vp]),
+    "kache_count_masked": (ctypes.c_int, [_vp, _vp, _vp, ctypes.c_size_t, ctypes.c_uint64, ctypes.c_uint64, _vp]),
+    "kache_sum": (ctypes.c_int, [_vp, _vp, _vp, ctypes.c_size_t, _vp]),
+    "kache_lookup": (ctypes.c_int, [_vp, _vp, _vp, ctypes.c_size_t, _vp, _vp, _vp]),
+    "kache_get": (ctypes.c_int, [_vp, ctypes.c_char_p, _u8p, _u64p]),
+    "kache_size": (ctypes.c_int, [_vp, _u64p]),
+    "kache_reduce": (ctypes.c_int, [_vp, ctypes.c_uint32, ctypes.c_uint64, ctypes.c_uint32, _u64p]),
+    "kache_for_each": (ctypes.c_int, [_vp, ctypes.c_uint32, ctypes.c_uint32, KEYS_FN, _vp]),
+    "kache_get_stats": (ctypes.c_int, [_vp, ctypes.POINTER(Stats)]),
+    "kache_strerror": (ctypes.c_char_p, [ctypes.c_int]),
+}
+
+
+def bind(L, sigs):
+    """Sets restype and argtypes of the library's functions named in `sigs`."""
+    for name, (res, args) in sigs.items():
+        f = getattr(L, name)
+        f.restype, f.argtypes = res, args
+    return L
+
+
 _lib = None
 
 
@@ -64,25 +95,8 @@ def lib():
         if not os.path.exists(LIB_PATH):
             raise RuntimeError(f"the CUDA library is not built: {LIB_PATH} is missing (run __graft_entry__.build())")
         L = ctypes.CDLL(LIB_PATH)
-        sig = {
-            "kache_supports": (ctypes.c_int, [ctypes.c_uint32, ctypes.c_uint32]),
-            "kache_default_options": (Options, [ctypes.c_uint32, ctypes.c_uint32]),
-            "kache_new": (ctypes.c_int, [ctypes.POINTER(Options), ctypes.POINTER(_vp)]),
-            "kache_free": (None, [_vp]),
-            "kache_register": (ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_uint32)]),
-            "kache_insert": (ctypes.c_int, [_vp, ctypes.c_uint32, _vp, _vp, ctypes.c_size_t, ctypes.c_uint32, ctypes.c_uint64, _u64p]),
-            "kache_insert_oriented": (ctypes.c_int, [_vp, ctypes.c_uint32, _vp, _vp, ctypes.c_size_t, ctypes.c_uint32, ctypes.c_uint64, ctypes.c_uint64, _u64p]),
-            "kache_update": (ctypes.c_int, [_vp, _vp, _vp, ctypes.c_size_t, ctypes.c_uint32, ctypes.c_uint64, _u64p]),
-            "kache_count": (ctypes.c_int, [_vp, _vp, _vp, ctypes.c_size_t, _vp]),
-            "kache_count_masked": (ctypes.c_int, [_vp, _vp, _vp, ctypes.c_size_t, ctypes.c_uint64, ctypes.c_uint64, _vp]),
-            "kache_sum": (ctypes.c_int, [_vp, _vp, _vp, ctypes.c_size_t, _vp]),
-            "kache_lookup": (ctypes.c_int, [_vp, _vp, _vp, ctypes.c_size_t, _vp, _vp, _vp]),
-            "kache_get": (ctypes.c_int, [_vp, ctypes.c_char_p, _u8p, _u64p]),
-            "kache_size": (ctypes.c_int, [_vp, _u64p]),
-            "kache_reduce": (ctypes.c_int, [_vp, ctypes.c_uint32, ctypes.c_uint64, ctypes.c_uint32, _u64p]),
-            "kache_for_each": (ctypes.c_int, [_vp, ctypes.c_uint32, ctypes.c_uint32, KEYS_FN, _vp]),
-            "kache_get_stats": (ctypes.c_int, [_vp, ctypes.POINTER(Stats)]),
-            "kache_strerror": (ctypes.c_char_p, [ctypes.c_int]),
+        sig = dict(CAPI_SIGS)
+        sig.update({
             "kache_b200_new": (ctypes.c_int, [ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint64, ctypes.c_double, ctypes.c_uint32, ctypes.POINTER(_vp)]),
             "kache_b200_set_stream": (ctypes.c_int, [_vp, _vp]),
             "kache_b200_upsert": (ctypes.c_int, [_vp, ctypes.c_uint32, _vp, _vp, ctypes.c_size_t, ctypes.c_uint32, ctypes.c_uint64, ctypes.c_uint64, _u64p]),
@@ -112,11 +126,8 @@ def lib():
             "kache_b200_server_wait": (ctypes.c_int, [_vp, ctypes.c_uint64, _u64p, ctypes.POINTER(ctypes.c_double)]),
             "kache_b200_server_stats": (ctypes.c_int, [_vp, _u64p, _u64p]),
             "kache_b200_memory_roof": (ctypes.c_int, [ctypes.c_uint64, ctypes.c_uint32, ctypes.c_uint64, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)]),
-        }
-        for name, (res, args) in sig.items():
-            f = getattr(L, name)
-            f.restype, f.argtypes = res, args
-        _lib = L
+        })
+        _lib = bind(L, sig)
     return _lib
 
 
@@ -183,11 +194,21 @@ class Table:
             _check(L.kache_b200_new(k, l, value_bytes, expected_keys, load_factor, 1 if pow2 else 0, ctypes.byref(h)), "kache_b200_new")
         self.h, self.k, self.l, self.vb = h, k, l, value_bytes
         self.vdt = self.VDT.get(value_bytes, np.uint8)
+        self.owned = True
+
+    @classmethod
+    def view(cls, h, k, l, value_bytes):
+        """A table owned elsewhere (a counter's): usable for queries, never freed through this object."""
+        t = cls.__new__(cls)
+        t.h, t.k, t.l, t.vb = _vp(h), k, l, value_bytes
+        t.vdt = cls.VDT.get(value_bytes, np.uint8)
+        t.owned = False
+        return t
 
     def close(self):
-        if self.h:
+        if self.h and self.owned:
             lib().kache_free(self.h)
-            self.h = _vp()
+        self.h = _vp()
 
     def __del__(self):
         try:
@@ -438,6 +459,10 @@ class Counter:
         r = ctypes.c_uint64()
         _check(lib().kache_counter_size(self.h, ctypes.byref(r)), "kache_counter_size")
         return r.value
+
+    def table(self):
+        """The counter's <31, u32, 22> table, for queries (owned by the counter)."""
+        return Table.view(lib().kache_counter_table(self.h), 31, 22, 4)
 
 
 def kernel_launches():

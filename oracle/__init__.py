@@ -57,6 +57,7 @@ class Oracle:
             "orc_dump": (_u64, [_vp, _vp, _vp]),
             "orc_reduce": (_u64, [_vp, ctypes.c_uint32, _u64]),
             "orc_histogram": (None, [_vp, _u64, _vp]),
+            "orc_digest": (None, [_vp, _vp, _u64, _vp]),
         }
         for name, (res, args) in sig.items():
             f = getattr(L, name)
@@ -156,6 +157,15 @@ class OracleTable:
         h = np.zeros(max_count + 1, np.uint64)
         self.o.orc_histogram(self.h, max_count, h.ctypes.data)
         return h
+
+
+def digest(keys, values=None):
+    """Order-independent digest of the (key, value) pairs of a dump (orc_digest): (count, sum1, sum2)."""
+    k = np.ascontiguousarray(keys, dtype=np.uint64)
+    v = None if values is None else np.ascontiguousarray(values, dtype=np.uint64)
+    out = np.zeros(3, np.uint64)
+    oracle().L.orc_digest(k.ctypes.data, None if v is None else v.ctypes.data, len(k), out.ctypes.data)
+    return tuple(int(x) for x in out)
 
 
 def describe(batch, k, l):
@@ -284,13 +294,47 @@ class RefTable:
     def capacity(self):
         return self.L.ref_capacity(self.h)
 
-    def dump(self):
+    def raw_dump(self):
+        """(keys, values) in the reference's for_each order; values None for a set."""
         n = self.size()
         keys = np.zeros(max(n, 1), np.uint64)
         vals = np.zeros(max(n, 1), np.uint64)
         c = self.L.ref_dump(self.h, keys.ctypes.data, vals.ctypes.data)
-        o = np.argsort(keys[:c], kind="stable")
-        return keys[:c][o], (vals[:c][o] if self.vb else None)
+        return keys[:c], (vals[:c] if self.vb else None)
+
+    def dump(self):
+        keys, vals = self.raw_dump()
+        o = np.argsort(keys, kind="stable")
+        return keys[o], (vals[o] if self.vb else None)
+
+    # The reference's benchmark drivers (ref_bench_*): batches of `batch` sequences over `threads` threads, each
+    # upserting thread a user of its own. Return (seconds, result).
+    def bench_upsert(self, b, op, x, threads, batch=64):
+        out = _u64()
+        s = self.L.ref_bench_upsert(self.h, *_b(b), batch, threads, op, x, ctypes.byref(out))
+        return s, out.value
+
+    def bench_update(self, b, op, x, threads, batch=64):
+        out = _u64()
+        s = self.L.ref_bench_update(self.h, *_b(b), batch, threads, op, x, ctypes.byref(out))
+        return s, out.value
+
+
+_ref_capi = None
+
+
+def ref_capi():
+    """The reference's own C interface (capi/*.cpp compiled by oracle/Makefile's `capi` target into
+    _ref/libkache_capi_ref.so) with the prototypes of kache_capi.h, or None where it was not built. Loaded with local
+    symbol binding, so it lives beside the B200 library in one process, each answering its own calls."""
+    global _ref_capi
+    if _ref_capi is None:
+        p = os.path.join(REF_DIR, "libkache_capi_ref.so")
+        if not os.path.exists(p):
+            return None
+        import kache
+        _ref_capi = kache.bind(ctypes.CDLL(p, mode=os.RTLD_LOCAL), kache.CAPI_SIGS)
+    return _ref_capi
 
 
 def replay_capacity(n, lf, pow2, inserted):

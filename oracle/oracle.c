@@ -508,3 +508,26 @@ void orc_replay_capacity(const uint64_t max_sz, const double lf, const int pow2,
         caps[i] = t.cap * B;
     }
 }
+
+/* Stafford's variant-13 finaliser, for the digest below. */
+static uint64_t dig_mix(uint64_t x)
+{
+    x ^= x >> 30, x *= 0xbf58476d1ce4e5b9ull;
+    x ^= x >> 27, x *= 0x94d049bb133111ebull;
+    return x ^ (x >> 31);
+}
+
+/* An order-independent digest of a multiset of (key, value) pairs, for comparing dumps too large to sort in a test:
+ * out[0] the pair count, out[1] and out[2] sums modulo 2^64 of two unrelated 64-bit mixes of each pair. Dumps of the
+ * same pairs in any order give the same digest; different ones agree only by chance. values may be NULL (a set). */
+void orc_digest(const uint64_t* keys, const uint64_t* values, const uint64_t n, uint64_t* out)
+{
+    uint64_t a = 0, b = 0;
+    for(uint64_t i = 0; i < n; ++i)
+    {
+        const uint64_t v = values ? values[i] : 0;
+        a += dig_mix(keys[i] ^ dig_mix(v + 0x632BE59BD9B4E019ull));
+        b += dig_mix((keys[i] + 0x9E3779B97F4A7C15ull) * 0xD1342543DE82EF95ull ^ dig_mix(v ^ 0x3C6EF372FE94F82Aull));
+    }
+    out[0] = n, out[1] = a, out[2] = b;
+}

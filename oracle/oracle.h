@@ -64,6 +64,9 @@ uint64_t orc_capacity(const orc_table* t);
 uint64_t orc_dump(const orc_table* t, uint64_t* keys, uint64_t* values);
 uint64_t orc_reduce(const orc_table* t, uint32_t what, uint64_t mask);
 void orc_histogram(const orc_table* t, uint64_t max, uint64_t* h);
+/* Order-independent digest of (key, value) pairs: out[0] the count, out[1..2] two sums of unrelated mixes; values may
+ * be NULL. For comparing dumps too large to sort. */
+void orc_digest(const uint64_t* keys, const uint64_t* values, uint64_t n, uint64_t* out);
 
 #ifdef __cplusplus
 }

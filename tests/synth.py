@@ -166,6 +166,26 @@ def config4(scale=1.0):
     return g, stretches(g, 150)
 
 
+# The served mix: a <31, u32, 22> map primed with a genome's 31-mers (2 Gbp at full size), then requests of 150 bp reads
+# with 1 % substitutions, upsert / find / count at 60/30/10, each of lognormal(2000 reads, sigma 1.5) clipped to
+# 1-1M reads, drawn from a pool of reads of the genome. Returns the genome, the priming pieces and (kind, batch) per
+# request (kind 0 upsert, 1 find, 2 count).
+def config5(scale=1.0, requests=300):
+    from kache import Batch
+    glen = int(2_000_000_000 * scale)
+    g = genome(glen, seed=51)
+    primer = stretches(g, 1_000_000)
+    pool = Batch(*reads_fixed(g, min(4_000_000, max(100_000, glen // 100)), 150, seed=52, sub=0.01, n_rate=0.0005))
+    rng = np.random.default_rng(53)
+    reqs = []
+    for _ in range(requests):
+        kind = rng.choice(3, p=[0.6, 0.3, 0.1])
+        m = int(np.clip(rng.lognormal(np.log(2000), 1.5), 1, min(1_000_000, pool.n)))
+        s = int(rng.integers(0, pool.n - m + 1))
+        reqs.append((int(kind), pool.slice(s, s + m)))
+    return g, primer, reqs
+
+
 # The benchmark workload of the headline metric: a map <31, u64, 22> sized for 10M keys; upsert(c + 1, init 1) of
 # 333,333 reads of 150 bp at 10x over a 5 Mbp genome (seed 1), then lookups of 1M held-out reads (seed 2).
 def config1(scale=1.0):

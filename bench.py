@@ -408,6 +408,11 @@ def run_b200(args):
         }
         cb = None if args.only_dev else cpu_baseline_sample(ins, held, min(128, os.cpu_count() or 1))
         line["cpu_baseline"] = cb
+        if ws == 1 and not args.only_dev and not args.no_sub:
+            line["cold_first_call"] = cold_first_call(dev, stream, d_ins_b.data_ptr(), d_ins_o.data_ptr(), bi.n, d_held_b.data_ptr(),
+                                                      d_held_o.data_ptr(), bh.n, d_found.data_ptr(), d_vals.data_ptr(), P)
+            line["config3_batched"] = sub_config3(dev, stream, local)
+            line["config5_served"] = sub_config5(dev, stream, local)
         print(json.dumps(line))
     T.close()
     if dist is not None:
@@ -415,13 +420,13 @@ def run_b200(args):
         dist.destroy_process_group()
 
 
-def run_density(kache, b):
+def run_density(kache, b, k=31):
     """Minimizer runs per k-mer position (rho): the share of positions whose minimizer hash differs from the previous
     position's in the same sequence, from the describer."""
-    t = kache.Table(31, 0, 1000)
+    t = kache.Table(k, 0, 1000, capi=(k == 31))
     key, h, cs, fwd, valid = t.describe(b)
     t.close()
-    pos = b.positions(31)
+    pos = b.positions(k)
     starts = np.zeros(len(h), bool)
     o = np.concatenate([[0], np.cumsum(pos)[:-1]]).astype(np.int64)
     starts[o[pos > 0]] = True
@@ -429,6 +434,262 @@ def run_density(kache, b):
     change[1:] = h[1:] != h[:-1]
     runs = (change | starts) & (valid == 1)
     return float(runs.sum()) / max(1, int(valid.sum()))
+
+
+# ---- Sub-records of the default line: the north-star forms beside the headline --------------------------------------
+
+def kernel_roofline(name, ms_total, launches, bytes_per_launch, A, peak, peak_kind):
+    """The roofline record of one kernel kind: algorithmic bytes per launch over its mean event-timed duration."""
+    per = ms_total / max(1, launches)
+    ach = bytes_per_launch / (per * 1e-3) / 1e9 if ms_total else None
+    return {"bound": "hbm", "kernel": name, "achieved": ach, "peak": peak, "unit": "GB/s",
+            "frac": (ach / peak) if ach else None, "peak_source": peak_kind, "launches": launches, "ms_total": ms_total,
+            "algorithmic_bytes_per_kmer": A, "bytes_per_launch": bytes_per_launch, "traffic": None,
+            "model": "A = b_in + b_out + 32*rho + 32*r_slot + 32*w_slot bytes per k-mer position"}
+
+
+def sub_config3(dev, stream, device_index):
+    """Config 3 at full size (strand map <27, u8, 16>, oriented upsert OR 1/2 then oriented find of every read), its
+    reads in batches of 256 as a caller of the plain per-call interface hands them over: one call per batch and kind
+    (the plain kernel), against the same batches as one kache_b200_run_dev_batches call per kind (the batched
+    persistent path: one segment list, one launch)."""
+    import torch
+    import kache
+    from kache import Batch
+    g, reads = synth.config3()
+    br = Batch(*reads)
+    P1 = positions(br.off, 27)
+    T = kache.Table(27, 1, 50_000_000, 0.8, False, capi=False)
+    T.set_stream(stream.cuda_stream)
+    u = T.register()
+    found = torch.empty(P1, dtype=torch.uint8, device=dev)
+    vals = torch.empty(P1, dtype=torch.uint8, device=dev)
+    fwd = torch.empty(P1, dtype=torch.uint8, device=dev)
+    pieces = dev_pieces(br, dev, 256)
+    starts = np.concatenate([[0], np.cumsum([int(np.maximum(np.diff(o_.cpu().numpy()) - 26, 0).sum()) for _, o_, _ in pieces])])
+    ups = [(b_.data_ptr(), o_.data_ptr(), n_) for b_, o_, n_ in pieces]
+    looks = [(b_.data_ptr(), o_.data_ptr(), n_, found[int(starts[i_]):].data_ptr(), vals[int(starts[i_]):].data_ptr(),
+              fwd[int(starts[i_]):].data_ptr()) for i_, (b_, o_, n_) in enumerate(pieces)]
+    torch.cuda.synchronize()
+
+    def step_plain():
+        T.clear()
+        for b_, o_, n_ in pieces:
+            T.upsert_oriented_dev(u, b_.data_ptr(), o_.data_ptr(), n_, kache.OR, 1, 2)
+        for i_, (b_, o_, n_) in enumerate(pieces):
+            at = int(starts[i_])
+            T.lookup_dev(b_.data_ptr(), o_.data_ptr(), n_, found[at:].data_ptr(), vals[at:].data_ptr(), fwd[at:].data_ptr())
+
+    def step_batched():
+        T.clear()
+        T.run_dev_batches(kache.RUN_UPSERT_ORIENTED, ups, kache.OR, 1, 2, u)
+        T.run_dev_batches(kache.RUN_LOOKUP, looks)
+
+    clocks = Clocks(device_index)
+    clocks.start()
+    ms_plain = timed_steps(stream, step_plain, 3, 3)
+    ms_b = timed_steps(stream, step_batched, 5, 3)
+    T.profile(True)
+    step_batched()
+    torch.cuda.synchronize()
+    prof = {kind: T.profile_read(i) for i, kind in enumerate(["upsert", "update", "lookup", "reduce", "resize", "other"])}
+    T.profile(False)
+    clk = clocks.stop()
+    inserted, cap = T.size(), T.capacity()
+    hit = float((found.cpu().numpy() == 1).sum()) / max(1, P1)
+    rho = run_density(kache, br.slice(0, 200), 27)
+    b_in = float(br.off[-1]) / P1
+    A_up = b_in + 32 * rho + 32 * (1 - inserted / P1) + 32 * 1.0
+    A_lk = b_in + 3 + 32 * rho + 32 * hit
+    peak, peak_kind = load_peaks()
+    kern = {"upsert_oriented": kernel_roofline("lane_kernel<27,16,Upsert_Visitor> (batched)", prof["upsert"][0], prof["upsert"][1],
+                                               A_up * P1 / max(1, prof["upsert"][1]), A_up, peak, peak_kind),
+            "lookup": kernel_roofline("stream_kernel<27,16,Lookup_Batches_Visitor> (batched)", prof["lookup"][0], prof["lookup"][1],
+                                      A_lk * P1 / max(1, prof["lookup"][1]), A_lk, peak, peak_kind)}
+    dom = max(kern, key=lambda k_: kern[k_]["ms_total"])
+    roof = dict(kern[dom])
+    roof["kernels"] = kern
+    T.close()
+    t_ref, threads = ref_sample(5, 50_000_000, 0.8, False, [("ref_bench_upsert_oriented", br, (3, 1, 2)), ("lookup", br, (27,))])
+    cpu = None if t_ref is None else {"value": 2 * P1 / t_ref, "unit": "k-mers/s", "cores": threads, "kind": "reference",
+                                      "sample": "the whole workload once: oriented upsert then per-position find, batches of 64 reads over the threads"}
+    return {"workload": f"config 3: {len(g)} bp genome, {br.n} reads lognormal(10 kb, 0.8) clipped 1-100 kb at 5x, 5% errors 3:1:1; "
+                        f"<27,u8,16> oriented upsert OR 1/2 then oriented find; {len(pieces)} batches of 256 reads",
+            "unit": "k-mers/s", "positions_per_step": 2 * P1, "keys": inserted, "capacity": cap,
+            "value": 2 * P1 / (ms_b * 1e-3), "ms_per_step": ms_b, "calls_per_step": 2, "form": "kache_b200_run_dev_batches per kind",
+            "plain": {"value": 2 * P1 / (ms_plain * 1e-3), "ms_per_step": ms_plain, "calls_per_step": 2 * len(pieces),
+                      "form": "one kache_b200_upsert_oriented_dev / kache_b200_lookup_dev call per batch"},
+            "batched_over_plain": ms_plain / ms_b, "target": ">= 2x the plain kernel's k-mers/s",
+            "kernel_ms_one_step": {k_: v_[0] for k_, v_ in prof.items()}, "roofline": roof, "cpu_baseline": cpu, "clocks": clk,
+            "l2": "inputs larger than L2 (reads 250 MB, table about 3 GB)"}
+
+
+def sub_config5(dev, stream, device_index, scale=0.05, requests=300):
+    """Config 5 at `scale` (a <31, u32, 22> map primed with a genome's 31-mers, then upsert ADD 1 / find / count requests
+    at 60/30/10, each of lognormal(2000, 1.5) 150 bp reads) with the requests resident in HBM: the batched persistent
+    path (one kache_b200_run_dev_batches call per kind), against the request server fed the same requests from four
+    client threads, at once (throughput) and at Poisson arrivals at 60 % of that rate (p50/p99 latency)."""
+    import torch
+    import kache
+    from kache import Batch
+    rng = np.random.default_rng(54)
+    g, primer, reqs = synth.config5(scale, requests)
+    T = kache.Table(31, 4, len(g), 0.8, False)
+    u = T.register()
+    ib, io, ni = dev_batch(Batch(*primer), dev)
+    T.upsert_dev(u, ib.data_ptr(), io.data_ptr(), ni, kache.KEEP, 0, 0)
+    torch.cuda.synchronize()
+    primed = T.size()
+    del ib, io
+    P = sum(int(b.positions(31).sum()) for _, b in reqs)
+    P_kind = [sum(int(b.positions(31).sum()) for k_, b in reqs if k_ == kind) for kind in range(3)]
+    T.set_stream(stream.cuda_stream)
+    dreq = []
+    for kind, b in reqs:
+        db, do, n_ = dev_batch(b, dev)
+        p_ = int(b.positions(31).sum())
+        o0 = torch.empty(max(p_, 1) if kind == 1 else max(n_, 1) * 8, dtype=torch.uint8, device=dev) if kind else None
+        o1 = torch.empty(max(p_, 1) * 4, dtype=torch.uint8, device=dev) if kind == 1 else None
+        dreq.append((kind, db, do, n_, o0, o1))
+    runs_dev = {kind: [(db.data_ptr(), do.data_ptr(), n_) + ((o0.data_ptr(),) if o0 is not None else ()) + ((o1.data_ptr(),) if o1 is not None else ())
+                       for k_, db, do, n_, o0, o1 in dreq if k_ == kind] for kind in range(3)}
+    res = {}
+
+    def dev_step():
+        res["ins"] = sum(T.run_dev_batches(kache.RUN_UPSERT, runs_dev[0], kache.ADD, 1, 1, u))
+        res["found"] = sum(T.run_dev_batches(kache.RUN_LOOKUP, runs_dev[1]))
+        T.run_dev_batches(kache.RUN_COUNT, runs_dev[2])
+
+    clocks = Clocks(device_index)
+    clocks.start()
+    dev_ms = timed_steps(stream, dev_step, 3, 3)
+    T.profile(True)
+    dev_step()
+    torch.cuda.synchronize()
+    prof = {kind: T.profile_read(i) for i, kind in enumerate(["upsert", "update", "lookup", "reduce", "resize", "other"])}
+    T.profile(False)
+    T.set_stream(None)
+    torch.cuda.synchronize()
+    S = kache.Server(T)
+
+    def serve_dev(arrivals=None):
+        tickets = [None] * len(dreq)
+        start = time.perf_counter()
+
+        def client(idx):
+            for i in idx:
+                if arrivals is not None:
+                    delay = start + arrivals[i] - time.perf_counter()
+                    if delay > 0:
+                        time.sleep(delay)
+                kind, db, do, n_, o0, o1 = dreq[i]
+                tickets[i] = S.submit_dev(kind, db.data_ptr(), do.data_ptr(), n_, op=kache.ADD, x=1, init=1,
+                                          out0=None if o0 is None else o0.data_ptr(), out1=None if o1 is None else o1.data_ptr())
+
+        th = [threading.Thread(target=client, args=(range(j, len(dreq), 4),)) for j in range(4)]
+        for t in th:
+            t.start()
+        for t in th:
+            t.join()
+        lat = [S.wait(t)[1] for t in tickets]
+        return time.perf_counter() - start, np.array(lat)
+
+    for _ in range(3):
+        serve_dev()     # warm-up
+    r0, _ = S.stats()
+    burst_s, burst_lat = serve_dev()
+    r1, _ = S.stats()
+    rate = 0.6 * len(dreq) / burst_s
+    open_s, open_lat = serve_dev(np.cumsum(rng.exponential(1.0 / rate, size=len(dreq))))
+    r2, _ = S.stats()
+    clk = clocks.stop()
+    S.close()
+    st = T.stats()
+    T.close()
+    del dreq, runs_dev
+    # Roofline of the batched form's dominant kernel: a map upsert writes a slot sector per position.
+    peak, peak_kind = load_peaks()
+    b_in = 150.0 / 120.0
+    rho = run_density(kache, reqs[0][1].slice(0, min(5000, reqs[0][1].n)))
+    hit = res["found"] / max(1, P_kind[1])
+    A_up = b_in + 32 * rho + 32 * (1 - res["ins"] / max(1, P_kind[0])) + 32 * 1.0
+    A_lk = b_in + 5 + 32 * rho + 32 * hit
+    A_ct = b_in + 32 * rho + 32 * hit
+    kern = {"upsert": kernel_roofline("lane_kernel<31,22,Upsert_Visitor> (batched)", prof["upsert"][0], prof["upsert"][1],
+                                      A_up * P_kind[0] / max(1, prof["upsert"][1]), A_up, peak, peak_kind),
+            "lookup": kernel_roofline("stream_kernel<31,22,Lookup_Batches_Visitor> (batched)", prof["lookup"][0], prof["lookup"][1],
+                                      A_lk * P_kind[1] / max(1, prof["lookup"][1]), A_lk, peak, peak_kind),
+            "count": kernel_roofline("lane_kernel<31,22,Seq_Reduce_Visitor> (batched)", prof["reduce"][0], prof["reduce"][1],
+                                     A_ct * P_kind[2] / max(1, prof["reduce"][1]), A_ct, peak, peak_kind)}
+    dom = max(kern, key=lambda k_: kern[k_]["ms_total"])
+    roof = dict(kern[dom])
+    roof["kernels"] = kern
+    cpu = cpu_served_reference(reqs, g, primer)
+    pct = lambda a, q: float(np.percentile(a, q))
+    return {"workload": f"config 5 at scale {scale}: {len(g)} bp genome primed ({primed} keys); {len(reqs)} requests of 150 bp "
+                        "reads (1% errors), lognormal(2000, 1.5) reads each clipped 1-1M, upsert ADD 1 / find / count at 60/30/10, "
+                        "resident in HBM", "unit": "k-mers/s", "positions": P,
+            "value": P / burst_s, "ms": 1000 * burst_s, "form": "request server, device requests from four threads at once",
+            "runs": r1 - r0, "p50_ms": pct(burst_lat, 50), "p99_ms": pct(burst_lat, 99),
+            "batched": {"value": P / (dev_ms * 1e-3), "ms": dev_ms, "calls": 3,
+                        "form": "kache_b200_run_dev_batches per kind (CUDA events)"},
+            "served_over_batched": (dev_ms * 1e-3) / burst_s, "target": "served within 20 % of the batched throughput",
+            "poisson": {"offered_requests_per_s": rate, "value": P / open_s, "p50_ms": pct(open_lat, 50),
+                        "p99_ms": pct(open_lat, 99), "runs": r2 - r1},
+            "kernel_ms_batched": {k_: v_[0] for k_, v_ in prof.items()}, "keys_after": st.keys, "capacity_after": st.capacity,
+            "roofline": roof, "cpu_baseline": cpu, "clocks": clk}
+
+
+def cpu_served_reference(reqs, g, primer, budget_s=20.0):
+    """The reference's table (oracle/_ref) primed with the same genome, then the requests served one at a time in
+    arrival order on one thread (upserts serialised with queries, as the reference's phase rule requires), until
+    `budget_s` seconds of request work are spent."""
+    import oracle
+    from kache import Batch
+    if oracle.ref() is None:
+        return None
+    R = oracle.RefTable(31, 4, len(g), 0.8, False, workers=min(128, os.cpu_count() or 1))
+    u = R.register()
+    R.bench_upsert(Batch(*primer), 0, 0, min(128, os.cpu_count() or 1))
+    done, P, t = 0, 0, 0.0
+    for kind, b in reqs:
+        t0 = time.perf_counter()
+        if kind == 0:
+            R.upsert(u, b, 2, 1)
+        elif kind == 1:
+            R.lookup(b)
+        else:
+            R.L.ref_count(R.h, b.bases.ctypes.data, b.off.ctypes.data, b.n)
+        t += time.perf_counter() - t0
+        P += int(b.positions(31).sum())
+        done += 1
+        if t > budget_s:
+            break
+    return {"value": P / t, "unit": "k-mers/s", "cores": 1, "kind": "reference",
+            "sample": f"the first {done} of {len(reqs)} requests in arrival order on one thread ({P} positions), "
+                      "after priming with all host threads"}
+
+
+def cold_first_call(dev, stream, d_ins_b, d_ins_o, n_ins, d_held_b, d_held_o, n_held, d_found, d_vals, P):
+    """Config 1 on a table just made by kache_new: the first upsert call grows the table from its creation size with
+    no rate learned from earlier calls, then the lookup; CUDA events around both calls."""
+    import torch
+    import kache
+    T = kache.Table(31, 8, N_KEYS, 0.8, False)
+    T.set_stream(stream.cuda_stream)
+    u = T.register()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    T.upsert_dev(u, d_ins_b, d_ins_o, n_ins, kache.ADD_WRAP, 1, 1)
+    T.lookup_dev(d_held_b, d_held_o, n_held, d_found, d_vals, None)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    keys = T.size()
+    T.close()
+    return {"value": P / (ms * 1e-3), "unit": "k-mers/s", "ms": ms, "keys": keys,
+            "form": "config 1's upsert then find, once, on a fresh kache_new table (no earlier call to learn from)"}
 
 
 # ---- The other workloads: one JSON line each, for the record (the default line is config 1) -----------------------
@@ -913,6 +1174,8 @@ def main():
     ap.add_argument("--requests", type=int, default=300, help="requests of configuration 5")
     ap.add_argument("--only-dev", action="store_true",
                     help="time the device-resident steps only (no e2e, CPU baseline or clock sampling): the profiling case")
+    ap.add_argument("--no-sub", action="store_true",
+                    help="leave out the sub-records of the default line (config 3 batched, config 5 served, cold first call)")
     args = ap.parse_args()
     if args.config != 1:
         {2: run_config2, 3: run_config3, 4: run_config4, 5: run_config5}[args.config](args)

@@ -54,6 +54,7 @@ def build(force=False, verbose=False):
         if r.returncode != 0:
             raise RuntimeError(f"link failed:\n{r.stderr}")
     build_facade_check(headers, force)
+    build_counter_check(force)
     return LIB
 
 
@@ -69,6 +70,24 @@ def build_facade_check(headers, force=False):
     r = subprocess.run(cmd, capture_output=True, text=True)
     if r.returncode != 0:
         raise RuntimeError(f"nvcc failed on {src}:\n{r.stderr}")
+    return exe
+
+
+def build_counter_check(force=False):
+    """The counter's C++ surface's check program (tests/counter_check.cpp): plain C++ over include/Kmer_Set_Counter.hpp,
+    linked against the library as a C++ caller of the reference's counter would be."""
+    src = os.path.join(ROOT, "tests", "counter_check.cpp")
+    exe = os.path.join(OUT, "counter_check")
+    hdr = os.path.join(ROOT, "include", "Kmer_Set_Counter.hpp")
+    if not os.path.exists(src):
+        return None
+    if not force and os.path.exists(exe) and os.path.getmtime(exe) >= max(os.path.getmtime(src), os.path.getmtime(hdr), os.path.getmtime(LIB)):
+        return exe
+    cmd = [os.environ.get("CXX", "g++"), "-std=c++20", "-O2", "-Wall", "-I" + os.path.join(ROOT, "include"), src, "-o", exe,
+           "-L" + OUT, "-lkache_b200", "-Wl,-rpath=" + OUT, "-pthread"]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError(f"g++ failed on {src}:\n{r.stderr}")
     return exe
 
 

@@ -92,3 +92,21 @@ def test_no_cpu_fallback_without_gpu():
     with pytest.raises(kache.KacheError) as e:
         kache.Table(31, 8, 1000)
     assert e.value.code == kache.KACHE_EINTERNAL
+
+
+def test_exports_the_counter_class():
+    """The counter's C++ surface (include/Kmer_Set_Counter.hpp): every member of the reference's class is exported by
+    the library, with the reference's signatures (counter/Kmer_Set_Counter.hpp:41-74)."""
+    import subprocess
+    lib = os.path.join(ROOT, "kache-hash_b200", "_build", "libkache_b200.so")
+    out = subprocess.run(["nm", "-DC", "--defined-only", lib], capture_output=True, text=True, check=True).stdout
+    for sig in ("kache_hash::Kmer_Set_Counter::supports(unsigned short)",
+                "kache_hash::Kmer_Set_Counter::Kmer_Set_Counter(unsigned short, unsigned long, unsigned long, double)",
+                "kache_hash::Kmer_Set_Counter::~Kmer_Set_Counter()",
+                "kache_hash::Kmer_Set_Counter::prime(std::__cxx11::basic_string<char, std::char_traits<char>, std::allocator<char> > const&)",
+                "kache_hash::Kmer_Set_Counter::count(std::__cxx11::basic_string<char, std::char_traits<char>, std::allocator<char> > const&)",
+                "kache_hash::Kmer_Set_Counter::histogram(unsigned long)",
+                "kache_hash::Kmer_Set_Counter::count_of(char const*) const",
+                "kache_hash::Kmer_Set_Counter::size() const",
+                "kache_hash::Kmer_Set_Counter::timings() const"):
+        assert sig in out, sig

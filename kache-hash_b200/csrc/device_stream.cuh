@@ -268,7 +268,7 @@ struct Upsert_Visitor
         if constexpr(!set_)
             if((r == FOUND || r == FOUND_PENDING) && !fn.is_noop())
             {
-                if(r == FOUND_PENDING && !comm && !await_published(L))
+                if(r == FOUND_PENDING && !comm && !await_published(L, T.wait_polls))
                     atomicOr(T.err, ERR_WAIT);
                 fn.apply(L.val, d.fwd);
             }

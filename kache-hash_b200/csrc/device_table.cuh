@@ -39,7 +39,10 @@ struct Dev_Table
     uint32_t ov_probe;      // Most slots an overflow probe visits.
     unsigned long long* ov_count;   // Keys in the overflow table.
     unsigned int* err;      // Nonzero after a bounded wait gave up.
+    uint32_t wait_polls;    // Most polls of a wait for a racing insert's publication.
 };
+
+constexpr uint32_t default_wait_polls = 1u << 22;
 
 constexpr uint32_t ERR_WAIT = 1;    // A wait for a racing insert's publication ran out.
 
@@ -417,10 +420,10 @@ __device__ __forceinline__ void publish(const Landing& L, const bool fence)
         *reinterpret_cast<volatile unsigned long long*>(L.ready) = 1ull;
 }
 
-// Waits, boundedly, for a racing insert of the same key to publish. Returns false if the wait ran out.
-__device__ __forceinline__ bool await_published(const Landing& L)
+// Waits, boundedly (`polls` polls), for a racing insert of the same key to publish. Returns false if the wait ran out.
+__device__ __forceinline__ bool await_published(const Landing& L, const uint32_t polls)
 {
-    for(uint32_t t = 0; t < (1u << 22); ++t)
+    for(uint32_t t = 0; t < polls; ++t)
     {
         if(L.cs ? ld_volatile_u8(L.cs) != 0 : *reinterpret_cast<const volatile unsigned long long*>(L.ready) != 0)
         {
@@ -509,6 +512,22 @@ __device__ __forceinline__ unsigned long long* find_chain(const Dev_Table& T, co
 {
     unsigned long long val;
     return find_chain<set_, cg_>(T, key, h, c, val, bc);
+}
+
+// For failure-injection tests: claims a slot of the key's primary bucket for it, as a racing inserter would, and
+// leaves it unpublished (its checksum stays 0), so that a later inserter of the key that must see its value first
+// waits on it. One thread; *ok is set to 1 if a slot was claimed.
+template <int k, int l, bool set_>
+__global__ void plant_claim_kernel(const Dev_Table T, const uint64_t key, unsigned long long* ok)
+{
+    const uint64_t b = bucket_of(minimizer_hash<k, l>(key), T.cap);
+    const uint4 c0 = *reinterpret_cast<const uint4*>(T.cs + b * B), c1 = *reinterpret_cast<const uint4*>(T.cs + b * B + 16);
+    const uint32_t empty = match32(c0, c1, 0);
+    *ok = 0;
+    if(!empty)
+        return;
+    unsigned long long* kw = key_word<set_>(T, b, __ffs(empty) - 1);
+    *ok = atomicCAS(kw, 0ull, ~key) == 0ull;
 }
 
 // The value of a found key, as read with it.

@@ -73,6 +73,11 @@ struct kache_table
     virtual cudaStream_t stream() const = 0;
     virtual void profile(bool on) = 0;
     virtual void profile_read(uint32_t kind, double& ms, uint64_t& launches) = 0;
+    // Failure injection for tests: the bound of the kernels' waits for a racing insert's publication, and a claim of
+    // the canonical k-mer `key`'s slot left unpublished, as by an inserter that never finishes. Returns whether a slot
+    // was claimed (its primary bucket had room).
+    virtual void testing_wait_polls(uint32_t polls) = 0;
+    virtual bool testing_plant_claim(uint64_t key) = 0;
 };
 
 namespace kache_b200
@@ -97,6 +102,23 @@ inline void check(const cudaError_t e, const char* what)
 }
 
 std::atomic<uint64_t>& launches();
+
+// Failure injection for tests: while nonnegative, the countdown of the library's device and page-locked allocations
+// before one fails as out of memory (0: the next one); -1 when off.
+std::atomic<int64_t>& alloc_fail_countdown();
+
+// Fails the allocation about to be made if the injected countdown reaches it.
+inline void alloc_gate()
+{
+    auto& c = alloc_fail_countdown();
+    for(int64_t v = c.load(); v >= 0; )
+        if(c.compare_exchange_weak(v, v - 1))
+        {
+            if(v == 0)
+                throw std::bad_alloc();
+            return;
+        }
+}
 
 // ---- Sizing, as the reference's (include/Streaming_Kmer_Hash_Table.hpp:383, 800-804, 1004-1011) ----------------
 
@@ -148,6 +170,7 @@ struct Dev_Buf
         if(n <= bytes)
             return;
         release();
+        alloc_gate();
         check(cudaMalloc(&p, std::max<size_t>(n, 256)), "cudaMalloc");
         bytes = std::max<size_t>(n, 256);
     }
@@ -180,6 +203,7 @@ struct Pinned_Buf
             return;
         const size_t m = std::max<size_t>({n + n / 4, 2 * bytes, size_t(1) << 20});
         release();
+        alloc_gate();
         check(cudaHostAlloc(&p, m, cudaHostAllocDefault), "cudaHostAlloc");
         bytes = m;
     }
@@ -376,6 +400,7 @@ class Engine final : public kache_table
     int sm_count_ = 148;
     Dev_Table epoch_T_{};   // The arrays epoch() last saw, and its count of changes.
     uint64_t epoch_ = 0;
+    uint32_t wait_polls_ = default_wait_polls;
 
     // The table.
     Dev_Buf cs_, spill_, slots_, ov_, ctr_;
@@ -469,6 +494,8 @@ class Engine final : public kache_table
         check(cudaMemsetAsync(slots.p, 0, cap * B * slot_bytes, stream_), "memset");
     }
 
+    static void swap_bufs(Dev_Buf& a, Dev_Buf& b) { std::swap(a.p, b.p), std::swap(a.bytes, b.bytes); }
+
     // Overflow capacity for n keys at load 0.8, a power of 2 (include/Concurrent_Hash_Table.hpp:157-172).
     static uint64_t ov_slots_for(const uint64_t n) { return ceil_pow2(static_cast<uint64_t>(std::ceil(static_cast<double>(n) / 0.8))); }
 
@@ -486,6 +513,7 @@ class Engine final : public kache_table
         T.cs = cs.as<uint8_t>(), T.spill = spill.as<uint32_t>(), T.slots = slots.as<unsigned long long>(), T.cap = cap;
         T.ov_count = ctr() + 1;
         T.err = reinterpret_cast<unsigned int*>(ctr() + 2) + 1;
+        T.wait_polls = wait_polls_;
     }
 
     // Doubles the overflow table.
@@ -521,13 +549,14 @@ class Engine final : public kache_table
         const uint64_t ov_keys = read_ctr(2)[1];
         uint64_t ov_slots = ov_slots_for(std::max<uint64_t>({1024, new_cap, static_cast<uint64_t>(ov_keys * 1.5)}));
         set_ov(T2, ov, ov_slots);
+        // First phase: keys at their primary buckets move directly. Second phase: the others and the overflow
+        // table's keys, marked in `dretry_a_`, go through the insertion chain. Every allocation comes before the
+        // live table's state changes, so that a failed one leaves the table as it was.
+        const uint64_t main_slots = old_cap * B, total = main_slots + ov_slots_;
+        dretry_dirty_ = true;
+        dretry_a_.ensure(total / 8 + 8), dretry_b_.ensure(total / 8 + 8);
         // The keys move, so the overflow count starts over.
         check(cudaMemsetAsync(ctr() + 1, 0, sizeof(unsigned long long), stream_), "memset");
-
-        // First phase: keys at their primary buckets move directly. Second phase: the others and the overflow
-        // table's keys, marked in `dretry_a_`, go through the insertion chain.
-        const uint64_t main_slots = old_cap * B, total = main_slots + ov_slots_;
-        dretry_a_.ensure(total / 8 + 8), dretry_b_.ensure(total / 8 + 8);
         check(cudaMemsetAsync(dretry_a_.p, 0, main_slots / 8, stream_), "memset");
         // Every overflow slot is marked for the second phase, unless the overflow table holds no key.
         check(cudaMemsetAsync(dretry_a_.as<char>() + main_slots / 8, ov_keys ? 0xFF : 0, ov_slots_ / 8, stream_), "memset");
@@ -1015,7 +1044,7 @@ class Engine final : public kache_table
         {
             size_t free_b = 0, total_b = 0;
             check(cudaMemGetInfo(&free_b, &total_b), "cudaMemGetInfo");
-            const size_t held = size_ == 0 ? cs_.bytes + spill_.bytes + slots_.bytes + ov_.bytes : 0;
+            const size_t held = size_ == 0 ? cs2_.bytes + spill2_.bytes + slots2_.bytes + ov2_.bytes : 0;
             if(need + (size_t(1) << 30) > free_b + held)
                 return;
         }
@@ -1024,7 +1053,20 @@ class Engine final : public kache_table
             resize(rebuild_cap(target));
             return;
         }
-        alloc_table(cs_, spill_, slots_, target);
+        if(!allocated)
+        {
+            // Made in the spare arrays and swapped in, so that a failed allocation leaves the table as it was; the
+            // arrays given up become the spares.
+            alloc_table(cs2_, spill2_, slots2_, target);
+            ov2_.ensure(ov_slots * 32);
+            swap_bufs(cs_, cs2_), swap_bufs(spill_, spill2_), swap_bufs(slots_, slots2_), swap_bufs(ov_, ov2_);
+        }
+        else
+        {
+            check(cudaMemsetAsync(cs_.p, 0, target * B, stream_), "memset");
+            check(cudaMemsetAsync(spill_.p, 0, target * 32, stream_), "memset");
+            check(cudaMemsetAsync(slots_.p, 0, target * B * slot_bytes, stream_), "memset");
+        }
         bind(T_, cs_, spill_, slots_, target);
         ov_slots_ = ov_slots;
         set_ov(T_, ov_, ov_slots_);
@@ -1077,6 +1119,7 @@ class Engine final : public kache_table
             uint64_t ins = c[0];
             while(static_cast<uint32_t>(c[2]))
             {
+                dretry_dirty_ = true;   // Until the retries end with no bit left set (a failure may come first).
                 grow_overflow();
                 check(cudaMemsetAsync(ctr(), 0, 8, stream_), "memset");
                 check(cudaMemsetAsync(retried, 0, 4, stream_), "memset");
@@ -1714,6 +1757,24 @@ public:
         const uint64_t r = run_update(bi, fn);
         finish_tune();
         return r;
+    }
+
+    void testing_wait_polls(const uint32_t polls) override
+    {
+        std::lock_guard<std::mutex> g(work);
+        wait_polls_ = polls;
+        T_.wait_polls = polls;
+    }
+
+    bool testing_plant_claim(const uint64_t key) override
+    {
+        std::lock_guard<std::mutex> g(work);
+        unsigned long long* d = ctr() + 4;
+        launch(K_OTHER, [&](){ plant_claim_kernel<k, l, set_><<<1, 1, 0, stream_>>>(T_, key, d); });
+        auto* h = pin_ctr_.as<uint64_t>(0);
+        check(cudaMemcpyAsync(h, d, 8, cudaMemcpyDeviceToHost, stream_), "D2H");
+        sync();
+        return h[0] != 0;
     }
 
     Dev_Table device_table() const override { return T_; }

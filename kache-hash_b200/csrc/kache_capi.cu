@@ -5,6 +5,7 @@
 // KACHE_ENOMEM, anything else, a CUDA failure included, as KACHE_EINTERNAL).
 #include "engine.cuh"
 #include "kache_b200.h"
+#include "kache_b200_testing.h"
 
 #include <exception>
 #include <mutex>
@@ -17,6 +18,12 @@ std::atomic<uint64_t>& launches()
 {
     static std::atomic<uint64_t> n{0};
     return n;
+}
+
+std::atomic<int64_t>& alloc_fail_countdown()
+{
+    static std::atomic<int64_t> c{-1};
+    return c;
 }
 
 // The engine's instantiations, one translation unit per (k, l) (tables_<k>_<l>.cu).
@@ -480,6 +487,37 @@ int kache_b200_profile_read(kache_table* const t, const uint32_t kind, double* c
 uint64_t kache_b200_kernel_launches(void) noexcept
 {
     return kache_b200::launches().load();
+}
+
+int kache_b200_testing_fail_allocation(const int64_t after) noexcept
+{
+    kache_b200::alloc_fail_countdown().store(after < 0 ? -1 : after);
+    return KACHE_OK;
+}
+
+int kache_b200_testing_plant_claim(kache_table* const t, const char* const kmer, const uint32_t wait_polls) noexcept
+{
+    if(t == nullptr || kmer == nullptr)
+        return KACHE_EINVAL;
+    uint64_t f = 0, r = 0;
+    for(uint32_t i = 0; i < t->kmer_k; ++i)
+    {
+        const char c = static_cast<char>(kmer[i] | 0x20);
+        if(c != 'a' && c != 'c' && c != 'g' && c != 't')
+            return KACHE_EINVAL;
+        const uint64_t b = static_cast<uint64_t>(((kmer[i] >> 2) ^ (kmer[i] >> 1)) & 3);
+        f = (f << 2) | b;
+        r |= (3 - b) << (2 * i);
+    }
+    const uint64_t key = f < r ? f : r;
+    return guard([&]()
+    {
+        uint64_t v = 0;
+        if(t->get(kmer, v))
+            return KACHE_EINVAL;
+        t->testing_wait_polls(wait_polls);
+        return t->testing_plant_claim(key) ? KACHE_OK : KACHE_EINVAL;
+    });
 }
 
 }

@@ -126,6 +126,8 @@ def lib():
             "kache_b200_server_wait": (ctypes.c_int, [_vp, ctypes.c_uint64, _u64p, ctypes.POINTER(ctypes.c_double)]),
             "kache_b200_server_stats": (ctypes.c_int, [_vp, _u64p, _u64p]),
             "kache_b200_memory_roof": (ctypes.c_int, [ctypes.c_uint64, ctypes.c_uint32, ctypes.c_uint64, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)]),
+            "kache_b200_testing_fail_allocation": (ctypes.c_int, [ctypes.c_int64]),
+            "kache_b200_testing_plant_claim": (ctypes.c_int, [_vp, ctypes.c_char_p, ctypes.c_uint32]),
         })
         _lib = bind(L, sig)
     return _lib

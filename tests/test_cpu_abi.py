@@ -13,7 +13,7 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
 def declared():
     names = []
-    for h in ("kache_capi.h", "kache_b200.h"):
+    for h in ("kache_capi.h", "kache_b200.h", "kache_b200_testing.h"):
         src = open(os.path.join(ROOT, "include", h)).read()
         names += re.findall(r"\b(kache_\w+)\s*\([^;]*\)\s*KACHE_NOEXCEPT\s*;", src)
     return sorted(set(names))

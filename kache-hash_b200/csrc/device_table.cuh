@@ -289,6 +289,26 @@ __device__ __forceinline__ void bucket_cs(const Dev_Table& T, const uint64_t b, 
         *bc->lo = c0, *bc->hi = c1, bc->b = b;
 }
 
+// The claim scan of bucket b for a key absent from its published slots below j0, the first slot whose checksum was
+// empty when they were read: a compare-and-swap straight away (a slot with an empty checksum is most likely
+// unclaimed), whose result, if it fails, is the racing claimer's key. Claimed keys form a prefix of the bucket, so the
+// scan meets any claim of the key made since. Returns INSERTED, FOUND or FOUND_PENDING with the slot at `j_out`, or
+// NONE if the bucket is full without the key.
+template <bool set_>
+__device__ __forceinline__ uint32_t claim_scan(const Dev_Table& T, const uint64_t b, const unsigned long long key_st, const uint32_t j0, uint32_t& j_out)
+{
+    for(uint32_t j = j0; j < B; ++j)
+    {
+        unsigned long long* kw = key_word<set_>(T, b, j);
+        const unsigned long long cur = atomicCAS(kw, 0ull, key_st);
+        if(cur == 0)
+            return j_out = j, INSERTED;
+        if(cur == key_st)
+            return j_out = j, (ld_volatile_u8(T.cs + b * B + j) != 0 ? FOUND : FOUND_PENDING);
+    }
+    return NONE;
+}
+
 // Tries the bucket b for the key: its published candidates, then the claim scan. Returns FOUND, FOUND_PENDING or
 // INSERTED with the slot at `j`, or NONE if the bucket is full without the key. With a cache holding b, the cached
 // candidates are tried first; if none is the key, the checksums are read afresh (other lanes may have published it
@@ -320,24 +340,10 @@ __device__ __forceinline__ uint32_t bucket_upsert(const Dev_Table& T, const uint
             return j_out = j, FOUND;
     }
     const uint32_t empty = match32(c0, c1, 0);
-
-    // The claim scan: a compare-and-swap straight away (a slot with an empty checksum is most likely unclaimed), whose
-    // result, if it fails, is the racing claimer's key.
-    for(uint32_t j = empty ? __ffs(empty) - 1 : B; j < B; ++j)
-    {
-        unsigned long long* kw = key_word<set_>(T, b, j);
-        const unsigned long long cur = atomicCAS(kw, 0ull, key_st);
-        if(cur == 0)
-        {
-            if(bc)
-                reinterpret_cast<uint8_t*>(j < 16 ? bc->lo : bc->hi)[j & 15] = c;
-            return j_out = j, INSERTED;
-        }
-        if(cur == key_st)
-            return j_out = j, (ld_volatile_u8(csb + j) != 0 ? FOUND : FOUND_PENDING);
-    }
-
-    return NONE;
+    const uint32_t r = claim_scan<set_>(T, b, key_st, empty ? __ffs(empty) - 1 : B, j_out);
+    if(r == INSERTED && bc)
+        reinterpret_cast<uint8_t*>(j_out < 16 ? bc->lo : bc->hi)[j_out & 15] = c;
+    return r;
 }
 
 // Tries the overflow table. Returns FOUND, FOUND_PENDING or INSERTED with the slot index at `i_out`, or OV_FULL.
@@ -370,6 +376,41 @@ struct Landing
     uint8_t c;
 };
 
+// The landing at slot j of bucket b.
+template <bool set_>
+__device__ __forceinline__ void land_at(const Dev_Table& T, const uint64_t b, const uint32_t j, const uint8_t c, Landing& L)
+{
+    unsigned long long* kw = key_word<set_>(T, b, j);
+    L.val = set_ ? nullptr : kw + 1, L.cs = T.cs + b * B + j, L.ready = nullptr, L.c = c;
+}
+
+// The upsert chain past a full primary bucket b: mark b's spill filter, then the secondary buckets in order, then
+// the overflow table (include/Streaming_Kmer_Hash_Table.hpp:2455-2490).
+template <bool set_>
+__device__ __noinline__ uint32_t upsert_past_primary(const Dev_Table& T, const uint64_t b, const unsigned long long key_st, const uint64_t h, const uint8_t c, Landing& L)
+{
+    const uint32_t fp = filter_pos(h);
+    uint32_t* sw = T.spill + b * 8 + (fp >> 5);
+    const uint32_t bit = 1u << (fp & 31);
+    if(!(__ldcg(sw) & bit))
+        atomicOr(sw, bit);
+
+    uint64_t p, q;
+    secondaries(h, T.cap, p, q);
+    uint32_t j;
+    uint32_t r = bucket_upsert<set_>(T, p, key_st, c, j);
+    uint64_t at = p;
+    if(r == NONE)
+        r = bucket_upsert<set_>(T, q, key_st, c, j), at = q;
+    if(r != NONE)
+        return land_at<set_>(T, at, j, c, L), r;
+
+    uint64_t i;
+    r = overflow_upsert(T, key_st, i);
+    L.val = T.ov + 4 * i + 1, L.cs = nullptr, L.ready = T.ov + 4 * i + 2, L.c = c;
+    return r;
+}
+
 // The upsert chain of one k-mer (include/Streaming_Kmer_Hash_Table.hpp:2431-2490, lock-free): primary bucket; if
 // full, mark its spill filter, then the secondary buckets in order; then the overflow table.
 template <bool set_>
@@ -378,35 +419,10 @@ __device__ __forceinline__ uint32_t upsert_chain(const Dev_Table& T, const uint6
     const unsigned long long key_st = ~key;
     uint32_t j;
     const uint64_t b = bucket_of(h, T.cap);
-    uint32_t r = bucket_upsert<set_>(T, b, key_st, c, j, bc);
-    uint64_t at = b;
-    if(r == NONE)
-    {
-        const uint32_t fp = filter_pos(h);
-        uint32_t* sw = T.spill + b * 8 + (fp >> 5);
-        const uint32_t bit = 1u << (fp & 31);
-        if(!(__ldcg(sw) & bit))
-            atomicOr(sw, bit);
-
-        uint64_t p, q;
-        secondaries(h, T.cap, p, q);
-        r = bucket_upsert<set_>(T, p, key_st, c, j);
-        at = p;
-        if(r == NONE)
-            r = bucket_upsert<set_>(T, q, key_st, c, j), at = q;
-    }
-
+    const uint32_t r = bucket_upsert<set_>(T, b, key_st, c, j, bc);
     if(r != NONE)
-    {
-        unsigned long long* kw = key_word<set_>(T, at, j);
-        L.val = set_ ? nullptr : kw + 1, L.cs = T.cs + at * B + j, L.ready = nullptr, L.c = c;
-        return r;
-    }
-
-    uint64_t i;
-    r = overflow_upsert(T, key_st, i);
-    L.val = T.ov + 4 * i + 1, L.cs = nullptr, L.ready = T.ov + 4 * i + 2, L.c = c;
-    return r;
+        return land_at<set_>(T, b, j, c, L), r;
+    return upsert_past_primary<set_>(T, b, key_st, h, c, L);
 }
 
 // Publishes a claimed slot after its value is written.
@@ -436,49 +452,42 @@ __device__ __forceinline__ bool await_published(const Landing& L, const uint32_t
     return false;
 }
 
-// Finds a key: primary bucket; absent if it is not full, or if its spill filter does not mark the minimizer; else the
-// secondary buckets; then the overflow table iff both are full (include/Streaming_Kmer_Hash_Table.hpp:2548-2574).
-// Returns the value word (the key word for a set), or null if absent; a map's value word, read together with its key
-// in one 16-byte load, also goes to `val`.
+// Compares the key of the slot at kw (16-byte aligned for a map) with key_st (a stored, complemented key), keeping its
+// value in `val`.
 template <bool set_, bool cg_>
-__device__ __forceinline__ unsigned long long* find_chain(const Dev_Table& T, const uint64_t key, const uint64_t h, const uint8_t c, unsigned long long& val, Bucket_Cache* bc = nullptr)
+__device__ __forceinline__ bool slot_is(const unsigned long long* kw, const unsigned long long key_st, unsigned long long& val)
 {
-    const unsigned long long key_st = ~key;
-    // Compares the key of the slot at kw (16-byte aligned for a map), keeping its value.
-    const auto same = [&](const unsigned long long* kw) -> bool
+    if constexpr(set_)
+        return (cg_ ? ld_cg(kw) : *kw) == key_st;
+    else
     {
-        if constexpr(set_)
-            return (cg_ ? ld_cg(kw) : *kw) == key_st;
-        else
-        {
-            const ulonglong2 s = cg_ ? __ldcg(reinterpret_cast<const ulonglong2*>(kw)) : *reinterpret_cast<const ulonglong2*>(kw);
-            val = s.y;
-            return s.x == key_st;
-        }
-    };
-    const auto probe = [&](const uint64_t b, bool& full, Bucket_Cache* pc) -> unsigned long long*
-    {
-        uint4 c0, c1;
-        bucket_cs<cg_>(T, b, pc, c0, c1);
-        uint32_t cand = candidates32<false>(c0, c1, c);
-        while(cand)
-        {
-            const uint32_t j = candidate_slot(__ffs(cand) - 1);
-            cand &= cand - 1;
-            unsigned long long* kw = key_word<set_>(T, b, j);
-            if(same(kw))
-                return set_ ? kw : kw + 1;
-        }
-        full = (c1.w >> 24) != 0;   // Keys fill a bucket's slots in order: full iff its last checksum is set.
-        return nullptr;
-    };
+        const ulonglong2 s = cg_ ? __ldcg(reinterpret_cast<const ulonglong2*>(kw)) : *reinterpret_cast<const ulonglong2*>(kw);
+        val = s.y;
+        return s.x == key_st;
+    }
+}
 
-    const uint64_t b = bucket_of(h, T.cap);
-    bool full = false;
-    if(auto* r = probe(b, full, bc))
-        return r;
-    if(!full)
-        return nullptr;
+// The candidates of bucket b in `cand` (candidates32's bits), tried in order: the found key's value word (its key word
+// in a set), or null.
+template <bool set_, bool cg_>
+__device__ __forceinline__ unsigned long long* try_candidates(const Dev_Table& T, const uint64_t b, uint32_t cand, const unsigned long long key_st, unsigned long long& val)
+{
+    while(cand)
+    {
+        const uint32_t j = candidate_slot(__ffs(cand) - 1);
+        cand &= cand - 1;
+        unsigned long long* kw = key_word<set_>(T, b, j);
+        if(slot_is<set_, cg_>(kw, key_st, val))
+            return set_ ? kw : kw + 1;
+    }
+    return nullptr;
+}
+
+// A find past a full primary bucket b (include/Streaming_Kmer_Hash_Table.hpp:2555-2574): absent unless b's spill
+// filter marks the minimizer; else the secondary buckets; then the overflow table iff both are full.
+template <bool set_, bool cg_>
+__device__ __forceinline__ unsigned long long* find_past_primary(const Dev_Table& T, const uint64_t b, const unsigned long long key_st, const uint64_t h, const uint8_t c, unsigned long long& val)
+{
     const uint32_t fp = filter_pos(h);
     const uint32_t sw = cg_ ? __ldcg(T.spill + b * 8 + (fp >> 5)) : T.spill[b * 8 + (fp >> 5)];
     if(!((sw >> (fp & 31)) & 1))
@@ -487,10 +496,15 @@ __device__ __forceinline__ unsigned long long* find_chain(const Dev_Table& T, co
     uint64_t p, q;
     secondaries(h, T.cap, p, q);
     bool full_p = false, full_q = false;
-    if(auto* r = probe(p, full_p, nullptr))
-        return r;
-    if(auto* r = probe(q, full_q, nullptr))
-        return r;
+    for(int t = 0; t < 2; ++t)
+    {
+        const uint64_t s = t ? q : p;
+        uint4 c0, c1;
+        bucket_cs<cg_>(T, s, nullptr, c0, c1);
+        if(auto* r = try_candidates<set_, cg_>(T, s, candidates32<false>(c0, c1, c), key_st, val))
+            return r;
+        (t ? full_q : full_p) = (c1.w >> 24) != 0;
+    }
     if(!(full_p && full_q))
         return nullptr;
 
@@ -505,6 +519,24 @@ __device__ __forceinline__ unsigned long long* find_chain(const Dev_Table& T, co
             return nullptr;
     }
     return nullptr;
+}
+
+// Finds a key: primary bucket; absent if it is not full, or if its spill filter does not mark the minimizer; else the
+// secondary buckets; then the overflow table iff both are full (include/Streaming_Kmer_Hash_Table.hpp:2548-2574).
+// Returns the value word (the key word for a set), or null if absent; a map's value word, read together with its key
+// in one 16-byte load, also goes to `val`.
+template <bool set_, bool cg_>
+__device__ __forceinline__ unsigned long long* find_chain(const Dev_Table& T, const uint64_t key, const uint64_t h, const uint8_t c, unsigned long long& val, Bucket_Cache* bc = nullptr)
+{
+    const unsigned long long key_st = ~key;
+    const uint64_t b = bucket_of(h, T.cap);
+    uint4 c0, c1;
+    bucket_cs<cg_>(T, b, bc, c0, c1);
+    if(auto* r = try_candidates<set_, cg_>(T, b, candidates32<false>(c0, c1, c), key_st, val))
+        return r;
+    if((c1.w >> 24) == 0)   // Keys fill a bucket's slots in order: full iff its last checksum is set.
+        return nullptr;
+    return find_past_primary<set_, cg_>(T, b, key_st, h, c, val);
 }
 
 template <bool set_, bool cg_>

@@ -13,7 +13,8 @@ import os
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "_build", "libkache_b200.so")
+# The CUDA library: the in-tree build, or another build of it named by KACHE_B200_LIB.
+LIB_PATH = os.environ.get("KACHE_B200_LIB") or os.path.join(HERE, "_build", "libkache_b200.so")
 
 KACHE_OK, KACHE_EINVAL, KACHE_EUSERS, KACHE_ENOMEM, KACHE_EINTERNAL = range(5)
 KEEP, ASSIGN, ADD, OR, MIN, MAX = range(6)

@@ -22,7 +22,7 @@ namespace kache_b200
 constexpr int lane_block = 256;     // Threads per block of the lane kernel.
 
 template <int k, int l, typename Visitor>
-__global__ void __launch_bounds__(lane_block) lane_kernel(const Dev_Batch batch, const uint64_t seg_b, const uint64_t seg_e, unsigned long long* next, Visitor vis)
+__global__ void __launch_bounds__(lane_block, 4) lane_kernel(const Dev_Batch batch, const uint64_t seg_b, const uint64_t seg_e, unsigned long long* next, Visitor vis)
 {
     constexpr int w = k - l + 1;
     static_assert(k <= 32 && l <= k && w >= 1, "k-mers in a machine word");

@@ -219,87 +219,46 @@ struct Upsert_Visitor
     // candidates cost a re-read; measured slower than reading the sector each time (config-1 upsert 1.91 vs 1.74 ms).
     __device__ __forceinline__ void lane_cache(uint4*, uint4*) {}
 
-    // Software-pipelined as the lookups are (Lookup_Visitor): a k-mer's bucket checksums load when it is described
-    // (stage 1); its candidates and first empty slot come from them one k-mer later, with the first candidate's key
-    // (or the first empty slot) loading (stage 2); one k-mer after that it is found or claimed and its value applied
-    // (stage 3). Claiming from a checksum snapshot two k-mers old is as correct as from a fresh one: slots below the
-    // snapshot's first empty one were published then and did not hold the key, and claimed keys form a prefix, so
-    // the claim scan from there meets any claim of the key made since (by other lanes, or by this lane's k-mers in
-    // between, which it resolves in order, publishing first). The pipeline drains at the end of each segment.
-    // A pending k-mer's flags, checksum, first empty slot and position, packed in one word: bits 0-7 flags, 8-15 the
-    // checksum, 16-21 the first empty slot (32 for none), 22-63 the position in the batch's outputs.
-    enum : uint64_t { F_ACTIVE = 1, F_FWD = 2 };
-    static __device__ __forceinline__ uint8_t meta_c(const uint64_t m) { return static_cast<uint8_t>(m >> 8); }
-    static __device__ __forceinline__ uint32_t meta_j0(const uint64_t m) { return static_cast<uint32_t>(m >> 16) & 63; }
-    static __device__ __forceinline__ uint64_t meta_out(const uint64_t m) { return m >> 22; }
-    struct Stage1 { uint64_t key, h, meta; uint4 c0, c1; };
-    struct Stage2 { uint64_t key, h, meta; unsigned long long kw; uint32_t cand; };
-    Stage1 s1;
-    Stage2 s2;
-
-    __device__ __forceinline__ void reset() { s1.meta = 0, s2.meta = 0; }
-    __device__ __forceinline__ void begin() { ins = 0, reset(); }
-    __device__ __forceinline__ void begin(uint8_t*) { begin(); }
-    __device__ __forceinline__ void begin_segment(uint64_t) { reset(); }
-    __device__ __forceinline__ void end_segment(uint64_t, uint32_t) { drain(); }
-    __device__ __forceinline__ void lane_begin(uint64_t, bool) { lane_ins = 0, reset(); }
+    __device__ __forceinline__ void begin() { ins = 0; }
+    __device__ __forceinline__ void begin(uint8_t*) { ins = 0; }
+    __device__ __forceinline__ void begin_segment(uint64_t) {}
+    __device__ __forceinline__ void end_segment(uint64_t, uint32_t) {}
+    __device__ __forceinline__ void lane_begin(uint64_t, bool) { lane_ins = 0; }
     __device__ __forceinline__ void lane_end(const uint64_t q, const bool has)
     {
-        drain();
         if(per_seq && has && lane_ins)
             atomicAdd(per_seq + q, static_cast<unsigned long long>(lane_ins));
     }
 
-    // Stage 3: finds or claims s2's k-mer, applies its operation, counts it.
-    __device__ __forceinline__ void resolve()
+    __device__ __forceinline__ void visit(const Kmer_Desc& d, const uint32_t lane)
     {
-        const uint64_t m = s2.meta;
+        bool active = d.valid;
+        if(retry_in && active)
+        {
+            const uint64_t gpos = d.out;
+            active = (retry_in[gpos >> 5] >> (gpos & 31)) & 1;
+        }
+
         Landing L{};
         uint32_t r = NONE;
-        const bool fwd = (m & F_FWD) != 0;
-        if(m & F_ACTIVE)
-        {
-            const unsigned long long key_st = ~s2.key;
-            const uint64_t b = bucket_of(s2.h, T.cap);
-            uint32_t j = B;
-            if(s2.cand)
-            {
-                if(s2.kw == key_st)
-                    r = FOUND, j = candidate_slot(__ffs(s2.cand) - 1);
-                else
-                    for(uint32_t cand = s2.cand & (s2.cand - 1); cand; cand &= cand - 1)
-                    {
-                        const uint32_t jc = candidate_slot(__ffs(cand) - 1);
-                        if(ld_cg(key_word<set_>(T, b, jc)) == key_st)
-                        {
-                            r = FOUND, j = jc;
-                            break;
-                        }
-                    }
-            }
-            if(r == NONE)
-                r = claim_scan<set_>(T, b, key_st, meta_j0(m), j);
-            if(r != NONE)
-                land_at<set_>(T, b, j, meta_c(m), L);
-            else
-                r = upsert_past_primary<set_>(T, b, key_st, s2.h, meta_c(m), L);
-        }
+        if(active)
+            r = upsert_chain<set_>(T, d.key, d.h, d.c, L);
         const bool comm = fn.commutes();
         if(r == INSERTED)
         {
             if constexpr(!set_)
             {
                 if(comm)
-                    fn.apply_init(L.val, fwd);
+                    fn.apply_init(L.val, d.fwd);
                 else
-                    write_val<V>(L.val, fn.initial(fwd));
+                    write_val<V>(L.val, fn.initial(d.fwd));
             }
             publish(L, !set_ && !comm);
         }
         else if(r == OV_FULL)
         {
-            const uint64_t out = meta_out(m);
-            atomicOr(retry_out + (out >> 5), 1u << (out & 31));
+            const uint64_t gpos = d.out;
+            atomicOr(retry_out + (gpos >> 5), 1u << (gpos & 31));
             *retried = 1;
         }
         ins += __popc(__ballot_sync(0xFFFFFFFFu, r == INSERTED));
@@ -311,62 +270,10 @@ struct Upsert_Visitor
             {
                 if(r == FOUND_PENDING && !comm && !await_published(L, T.wait_polls))
                     atomicOr(T.err, ERR_WAIT);
-                fn.apply(L.val, fwd);
+                fn.apply(L.val, d.fwd);
             }
         if(r == INSERTED && !L.cs)
             atomicAdd(T.ov_count, 1ull);
-    }
-
-    // Stage 2: s1's candidates and first empty slot, from its checksums; the slot a compare or claim will touch first
-    // starts loading.
-    __device__ __forceinline__ Stage2 advance() const
-    {
-        Stage2 n;
-        n.key = s1.key, n.h = s1.h, n.meta = s1.meta;
-        n.cand = 0, n.kw = 0;
-        if(s1.meta & F_ACTIVE)
-        {
-            n.cand = candidates32<true>(s1.c0, s1.c1, meta_c(s1.meta));
-            const uint32_t empty = match32(s1.c0, s1.c1, 0);
-            const uint32_t j0 = empty ? __ffs(empty) - 1 : B;
-            n.meta |= uint64_t(j0) << 16;
-            const uint32_t jh = n.cand ? candidate_slot(__ffs(n.cand) - 1) : j0;
-            if(jh < B)
-                n.kw = ld_cg(key_word<set_>(T, bucket_of(s1.h, T.cap), jh));
-        }
-        return n;
-    }
-
-    __device__ __forceinline__ void step(const Stage1& n1)
-    {
-        const Stage2 n2 = advance();
-        resolve();
-        s2 = n2, s1 = n1;
-    }
-
-    __device__ __forceinline__ void drain()
-    {
-        Stage1 none;
-        none.meta = 0;
-        step(none);
-        step(none);
-    }
-
-    // Stage 1: the k-mer described (in retry mode, only if its position is marked), its bucket's checksums loading.
-    __device__ __forceinline__ void visit(const Kmer_Desc& d, const uint32_t)
-    {
-        bool active = d.valid;
-        if(retry_in && active)
-            active = (retry_in[d.out >> 5] >> (d.out & 31)) & 1;
-        Stage1 n;
-        n.key = d.key, n.h = d.h;
-        n.meta = (d.out << 22) | (uint64_t(d.c) << 8) | (active ? F_ACTIVE : 0) | (d.fwd ? F_FWD : 0);
-        if(active)
-        {
-            const uint8_t* csb = T.cs + bucket_of(d.h, T.cap) * B;
-            n.c0 = ld_cg4(csb), n.c1 = ld_cg4(csb + 16);
-        }
-        step(n);
     }
 
     __device__ __forceinline__ void end(const uint32_t lane) { warp_flush(inserted, ins, lane); }
@@ -414,13 +321,6 @@ struct Update_Visitor
 
 // Per-position lookup (capi/Kmer_Table.hpp:163-190): found (0 absent, 1 present, 2 not a k-mer), value, orientation
 // at pos_off[q] + i.
-//
-// Software-pipelined over the k-mers a lane is handed (rows of a warp's segment, or positions of a lane's segment):
-// a k-mer's bucket checksums are loaded when it is described (stage 1), its first candidate slot's key and value one
-// k-mer later (stage 2), and it is resolved and written one k-mer after that (stage 3). Each lane so keeps three k-mers'
-// loads in flight, and the describer's work on the next k-mers covers their latency instead of waiting on them one
-// by one. Rarer cases -- further candidates, a full primary bucket -- are resolved at stage 3 with plain loads. The
-// pipeline drains at the end of each segment, so it never spans two sequences' output offsets.
 template <bool set_, typename V>
 struct Lookup_Visitor
 {
@@ -431,106 +331,29 @@ struct Lookup_Visitor
     uint8_t* fwd;
     uint64_t obase;
 
-    // A pending k-mer's flags, checksum and output index, packed in one word: bits 0-7 flags, 8-15 the checksum,
-    // 22-63 the output index.
-    enum : uint64_t { F_VALID = 1, F_IN = 2, F_FWD = 4, F_FULL = 8 };
-    static __device__ __forceinline__ uint8_t meta_c(const uint64_t m) { return static_cast<uint8_t>(m >> 8); }
-    static __device__ __forceinline__ uint64_t meta_o(const uint64_t m) { return m >> 22; }
-    struct Stage1 { uint64_t key, h, meta; uint4 c0, c1; };
-    struct Stage2 { uint64_t key, h, meta; ulonglong2 kv; uint32_t cand; };
-    Stage1 s1;
-    Stage2 s2;
-
-    __device__ __forceinline__ void reset() { s1.meta = 0, s2.meta = 0; }
-    __device__ __forceinline__ void begin() { reset(); }
-    __device__ __forceinline__ void begin_segment(const uint64_t q) { obase = pos_off[q], reset(); }
-    __device__ __forceinline__ void end_segment(uint64_t, uint32_t) { drain(); }
-    __device__ __forceinline__ void lane_begin(const uint64_t q, const bool has) { obase = has ? pos_off[q] : 0, reset(); }
-    __device__ __forceinline__ void lane_end(uint64_t, bool) { drain(); }
+    __device__ __forceinline__ void begin() {}
+    __device__ __forceinline__ void begin_segment(const uint64_t q) { obase = pos_off[q]; }
+    __device__ __forceinline__ void end_segment(uint64_t, uint32_t) {}
+    __device__ __forceinline__ void lane_begin(const uint64_t q, const bool has) { obase = has ? pos_off[q] : 0; }
+    __device__ __forceinline__ void lane_end(uint64_t, bool) {}
     __device__ __forceinline__ void end(uint32_t) {}
     __device__ __forceinline__ void lane_cache(uint4*, uint4*) {}
 
-    // Stage 3: resolves the k-mer of s2 and writes its outputs.
-    __device__ __forceinline__ void resolve()
-    {
-        const uint64_t m = s2.meta;
-        if(!(m & F_IN))
-            return;
-        const unsigned long long key_st = ~s2.key;
-        unsigned long long w = 0;
-        bool hit = false;
-        if(m & F_VALID)
-        {
-            const uint64_t b = bucket_of(s2.h, T.cap);
-            if(s2.cand)
-            {
-                if(s2.kv.x == key_st)
-                    hit = true, w = s2.kv.y;
-                else
-                    hit = try_candidates<set_, false>(T, b, s2.cand & (s2.cand - 1), key_st, w) != nullptr;
-            }
-            if(!hit && (m & F_FULL))
-                hit = find_past_primary<set_, false>(T, b, key_st, s2.h, meta_c(m), w) != nullptr;
-        }
-        const uint64_t o = meta_o(m);
-        found[o] = (m & F_VALID) ? (hit ? 1 : 0) : 2;
-        if constexpr(!set_)
-            if(values)
-                values[o] = hit ? value_of<V>(w) : V(0);
-        if(fwd)
-            fwd[o] = (m & F_FWD) != 0;
-    }
-
-    // Stage 2: the candidates of s1's bucket, and the first one's slot loading.
-    __device__ __forceinline__ Stage2 advance() const
-    {
-        Stage2 n;
-        n.key = s1.key, n.h = s1.h, n.meta = s1.meta;
-        n.cand = 0, n.kv = make_ulonglong2(0, 0);
-        if(s1.meta & F_VALID)
-        {
-            n.cand = candidates32<false>(s1.c0, s1.c1, meta_c(s1.meta));
-            if((s1.c1.w >> 24) != 0)
-                n.meta |= F_FULL;
-            if(n.cand)
-            {
-                const unsigned long long* kw = key_word<set_>(T, bucket_of(s1.h, T.cap), candidate_slot(__ffs(n.cand) - 1));
-                if constexpr(set_)
-                    n.kv.x = *kw;
-                else
-                    n.kv = *reinterpret_cast<const ulonglong2*>(kw);
-            }
-        }
-        return n;
-    }
-
-    __device__ __forceinline__ void step(const Stage1& n1)
-    {
-        const Stage2 n2 = advance();
-        resolve();
-        s2 = n2, s1 = n1;
-    }
-
-    __device__ __forceinline__ void drain()
-    {
-        Stage1 none;
-        none.meta = 0;
-        step(none);
-        step(none);
-    }
-
-    // Stage 1: the k-mer described, its bucket's checksums loading.
     __device__ __forceinline__ void visit(const Kmer_Desc& d, const uint32_t)
     {
-        Stage1 n;
-        n.key = d.key, n.h = d.h;
-        n.meta = ((obase + d.pos) << 22) | (uint64_t(d.c) << 8) | (d.valid ? F_VALID : 0) | (d.in ? F_IN : 0) | (d.valid && d.fwd ? F_FWD : 0);
+        const unsigned long long* v = nullptr;
+        unsigned long long w = 0;
         if(d.valid)
-        {
-            const uint8_t* csb = T.cs + bucket_of(d.h, T.cap) * B;
-            n.c0 = *reinterpret_cast<const uint4*>(csb), n.c1 = *reinterpret_cast<const uint4*>(csb + 16);
-        }
-        step(n);
+            v = find_chain<set_, false>(T, d.key, d.h, d.c, w);
+        if(!d.in)
+            return;
+        const uint64_t o = obase + d.pos;
+        found[o] = d.valid ? (v ? 1 : 0) : 2;
+        if constexpr(!set_)
+            if(values)
+                values[o] = v ? value_of<V>(w) : V(0);
+        if(fwd)
+            fwd[o] = d.valid && d.fwd;
     }
 };
 

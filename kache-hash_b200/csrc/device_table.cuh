@@ -289,26 +289,6 @@ __device__ __forceinline__ void bucket_cs(const Dev_Table& T, const uint64_t b, 
         *bc->lo = c0, *bc->hi = c1, bc->b = b;
 }
 
-// The claim scan of bucket b for a key absent from its published slots below j0, the first slot whose checksum was
-// empty when they were read: a compare-and-swap straight away (a slot with an empty checksum is most likely
-// unclaimed), whose result, if it fails, is the racing claimer's key. Claimed keys form a prefix of the bucket, so the
-// scan meets any claim of the key made since. Returns INSERTED, FOUND or FOUND_PENDING with the slot at `j_out`, or
-// NONE if the bucket is full without the key.
-template <bool set_>
-__device__ __forceinline__ uint32_t claim_scan(const Dev_Table& T, const uint64_t b, const unsigned long long key_st, const uint32_t j0, uint32_t& j_out)
-{
-    for(uint32_t j = j0; j < B; ++j)
-    {
-        unsigned long long* kw = key_word<set_>(T, b, j);
-        const unsigned long long cur = atomicCAS(kw, 0ull, key_st);
-        if(cur == 0)
-            return j_out = j, INSERTED;
-        if(cur == key_st)
-            return j_out = j, (ld_volatile_u8(T.cs + b * B + j) != 0 ? FOUND : FOUND_PENDING);
-    }
-    return NONE;
-}
-
 // Tries the bucket b for the key: its published candidates, then the claim scan. Returns FOUND, FOUND_PENDING or
 // INSERTED with the slot at `j`, or NONE if the bucket is full without the key. With a cache holding b, the cached
 // candidates are tried first; if none is the key, the checksums are read afresh (other lanes may have published it
@@ -340,10 +320,24 @@ __device__ __forceinline__ uint32_t bucket_upsert(const Dev_Table& T, const uint
             return j_out = j, FOUND;
     }
     const uint32_t empty = match32(c0, c1, 0);
-    const uint32_t r = claim_scan<set_>(T, b, key_st, empty ? __ffs(empty) - 1 : B, j_out);
-    if(r == INSERTED && bc)
-        reinterpret_cast<uint8_t*>(j_out < 16 ? bc->lo : bc->hi)[j_out & 15] = c;
-    return r;
+
+    // The claim scan: a compare-and-swap straight away (a slot with an empty checksum is most likely unclaimed), whose
+    // result, if it fails, is the racing claimer's key.
+    for(uint32_t j = empty ? __ffs(empty) - 1 : B; j < B; ++j)
+    {
+        unsigned long long* kw = key_word<set_>(T, b, j);
+        const unsigned long long cur = atomicCAS(kw, 0ull, key_st);
+        if(cur == 0)
+        {
+            if(bc)
+                reinterpret_cast<uint8_t*>(j < 16 ? bc->lo : bc->hi)[j & 15] = c;
+            return j_out = j, INSERTED;
+        }
+        if(cur == key_st)
+            return j_out = j, (ld_volatile_u8(csb + j) != 0 ? FOUND : FOUND_PENDING);
+    }
+
+    return NONE;
 }
 
 // Tries the overflow table. Returns FOUND, FOUND_PENDING or INSERTED with the slot index at `i_out`, or OV_FULL.
@@ -376,41 +370,6 @@ struct Landing
     uint8_t c;
 };
 
-// The landing at slot j of bucket b.
-template <bool set_>
-__device__ __forceinline__ void land_at(const Dev_Table& T, const uint64_t b, const uint32_t j, const uint8_t c, Landing& L)
-{
-    unsigned long long* kw = key_word<set_>(T, b, j);
-    L.val = set_ ? nullptr : kw + 1, L.cs = T.cs + b * B + j, L.ready = nullptr, L.c = c;
-}
-
-// The upsert chain past a full primary bucket b: mark b's spill filter, then the secondary buckets in order, then
-// the overflow table (include/Streaming_Kmer_Hash_Table.hpp:2455-2490).
-template <bool set_>
-__device__ __noinline__ uint32_t upsert_past_primary(const Dev_Table& T, const uint64_t b, const unsigned long long key_st, const uint64_t h, const uint8_t c, Landing& L)
-{
-    const uint32_t fp = filter_pos(h);
-    uint32_t* sw = T.spill + b * 8 + (fp >> 5);
-    const uint32_t bit = 1u << (fp & 31);
-    if(!(__ldcg(sw) & bit))
-        atomicOr(sw, bit);
-
-    uint64_t p, q;
-    secondaries(h, T.cap, p, q);
-    uint32_t j;
-    uint32_t r = bucket_upsert<set_>(T, p, key_st, c, j);
-    uint64_t at = p;
-    if(r == NONE)
-        r = bucket_upsert<set_>(T, q, key_st, c, j), at = q;
-    if(r != NONE)
-        return land_at<set_>(T, at, j, c, L), r;
-
-    uint64_t i;
-    r = overflow_upsert(T, key_st, i);
-    L.val = T.ov + 4 * i + 1, L.cs = nullptr, L.ready = T.ov + 4 * i + 2, L.c = c;
-    return r;
-}
-
 // The upsert chain of one k-mer (include/Streaming_Kmer_Hash_Table.hpp:2431-2490, lock-free): primary bucket; if
 // full, mark its spill filter, then the secondary buckets in order; then the overflow table.
 template <bool set_>
@@ -419,10 +378,35 @@ __device__ __forceinline__ uint32_t upsert_chain(const Dev_Table& T, const uint6
     const unsigned long long key_st = ~key;
     uint32_t j;
     const uint64_t b = bucket_of(h, T.cap);
-    const uint32_t r = bucket_upsert<set_>(T, b, key_st, c, j, bc);
+    uint32_t r = bucket_upsert<set_>(T, b, key_st, c, j, bc);
+    uint64_t at = b;
+    if(r == NONE)
+    {
+        const uint32_t fp = filter_pos(h);
+        uint32_t* sw = T.spill + b * 8 + (fp >> 5);
+        const uint32_t bit = 1u << (fp & 31);
+        if(!(__ldcg(sw) & bit))
+            atomicOr(sw, bit);
+
+        uint64_t p, q;
+        secondaries(h, T.cap, p, q);
+        r = bucket_upsert<set_>(T, p, key_st, c, j);
+        at = p;
+        if(r == NONE)
+            r = bucket_upsert<set_>(T, q, key_st, c, j), at = q;
+    }
+
     if(r != NONE)
-        return land_at<set_>(T, b, j, c, L), r;
-    return upsert_past_primary<set_>(T, b, key_st, h, c, L);
+    {
+        unsigned long long* kw = key_word<set_>(T, at, j);
+        L.val = set_ ? nullptr : kw + 1, L.cs = T.cs + at * B + j, L.ready = nullptr, L.c = c;
+        return r;
+    }
+
+    uint64_t i;
+    r = overflow_upsert(T, key_st, i);
+    L.val = T.ov + 4 * i + 1, L.cs = nullptr, L.ready = T.ov + 4 * i + 2, L.c = c;
+    return r;
 }
 
 // Publishes a claimed slot after its value is written.

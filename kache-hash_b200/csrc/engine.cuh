@@ -309,36 +309,60 @@ inline bool host_acgt(const char c)
 
 // ---- The lane kernel's autotuner ---------------------------------------------------------------------------------
 
-// Picks the lane kernel's segment length -- positions per lane, which sets how many lanes a batch has and how much of
-// each lane's rolling is warm-up -- per operation (upsert, update, per-sequence reduction) and batch size class (the
-// log2 of its positions), online: the first calls of a class try each candidate, in turn from the built-in choice;
-// later calls take the fastest per position (a moving average of the measured kernel time), and every 64th call
-// retries another candidate so the averages follow the table as it fills.
+// Picks the lane kernel's launch shape per operation (upsert, update, per-sequence reduction) and batch size class (the
+// log2 of its positions), online, over two dimensions:
+//   - the segment length, positions per lane: how many lanes a batch has and how much of each lane's rolling is
+//     warm-up (k - 1 bases per segment);
+//   - the blocks launched per SM, which take segments from the work counter: how many of the kernel's warps are
+//     resident at once against how long the last ones run alone.
+// Candidate c is segment length len[c % 4] at blocks[c / 4] per SM. The first calls of a class search coordinate by
+// coordinate: every segment length at the built-in block count, then every block count at the best length so far.
+// Later calls take the fastest per position (a moving average of the event-timed kernel time), and every 64th call
+// retries a neighbour of the best so the averages follow the table as it fills.
 class Seg_Tuner
 {
 public:
-    static constexpr int cands = 4;
-    static constexpr uint32_t len[cands] = {16, 32, 64, 128};
+    static constexpr int lens = 4, grids = 4, cands = lens * grids;
+    static constexpr uint32_t len[lens] = {16, 32, 64, 128};
+    static constexpr uint32_t blocks[grids] = {16, 8, 4, 2};    // Per SM; the first is the built-in count.
 
-    // The candidate for a call of `kind` over `pos` positions; `dflt` is the built-in choice.
+    static uint32_t seg_len_of(const int c) { return len[c % lens]; }
+    static uint32_t blocks_of(const int c) { return blocks[c / lens]; }
+
+    // The candidate for a call of `kind` over `pos` positions; `dflt` is the built-in segment length.
     int pick(const int kind, const uint64_t pos, const uint32_t dflt)
     {
         Slot& s = slot(kind, pos);
         int d = 0;
-        while(d + 1 < cands && len[d] < dflt)
+        while(d + 1 < lens && len[d] < dflt)
             d++;
-        for(int i = 0; i < cands; ++i)
+        for(int i = 0; i < lens; ++i)       // First coordinate: segment lengths at the built-in block count.
         {
-            const int c = (d + i) % cands;
+            const int c = (d + i) % lens;
             if(s.tries[c] == 0)
                 return c;
         }
-        int best = 0;
-        for(int c = 1; c < cands; ++c)
-            if(s.ns_per_pos[c] < s.ns_per_pos[best])
+        int best_len = 0;
+        for(int c = 1; c < lens; ++c)
+            if(s.ns_per_pos[c] < s.ns_per_pos[best_len])
+                best_len = c;
+        for(int g = 1; g < grids; ++g)      // Second: block counts at the best length.
+            if(s.tries[g * lens + best_len] == 0)
+                return g * lens + best_len;
+        int best = best_len;
+        for(int c = 0; c < cands; ++c)
+            if(s.tries[c] > 0 && s.ns_per_pos[c] < s.ns_per_pos[best])
                 best = c;
         if(++s.calls % 64 == 0)
-            return (best + 1 + static_cast<int>(s.calls / 64) % (cands - 1)) % cands;
+        {
+            // A neighbour of the best in one coordinate, in turn.
+            const int turn = static_cast<int>(s.calls / 64) % 4;
+            const int l = best % lens, g = best / lens;
+            if(turn == 0 && l + 1 < lens) return g * lens + l + 1;
+            if(turn == 1 && l > 0) return g * lens + l - 1;
+            if(turn == 2 && g + 1 < grids) return (g + 1) * lens + l;
+            if(turn == 3 && g > 0) return (g - 1) * lens + l;
+        }
         return best;
     }
 
@@ -641,7 +665,7 @@ class Engine final : public kache_table
             return last_seg_len_[tune_kind_];     // Before counting: likely the length this kind's last call used.
         tune_cand_ = tuner_.pick(tune_kind_, total_pos, builtin_seg_len(total_pos));
         tune_pos_ = total_pos;
-        return last_seg_len_[tune_kind_] = Seg_Tuner::len[tune_cand_];
+        return last_seg_len_[tune_kind_] = Seg_Tuner::seg_len_of(tune_cand_);
     }
 
     // Starts a tuned call of `kind` (0 upsert, 1 update, 2 per-sequence reduction); finish_tune() records it.
@@ -934,10 +958,11 @@ class Engine final : public kache_table
             launch(kind, [&](){ stream_kernel<k, l, Vis><<<grid_for(se - sb, stream_warps), 32 * stream_warps, 0, stream_>>>(bi.b, sb, se, vis); });
             return;
         }
-        const uint64_t blocks = std::min<uint64_t>((se - sb + lane_block - 1) / lane_block, uint64_t(sm_count_) * 16);
+        const bool timed = tune_kind_ >= 0 && tune_cand_ >= 0;
+        const uint64_t per_sm = timed ? Seg_Tuner::blocks_of(tune_cand_) : Seg_Tuner::blocks[0];
+        const uint64_t blocks = std::min<uint64_t>((se - sb + lane_block - 1) / lane_block, uint64_t(sm_count_) * per_sm);
         unsigned long long* next = ctr() + 7;     // The lane kernel's work counter.
         check(cudaMemsetAsync(next, 0, sizeof(unsigned long long), stream_), "memset");
-        const bool timed = tune_kind_ >= 0 && tune_cand_ >= 0;
         if(timed)
         {
             if(tune_used_ == tune_ev_.size())

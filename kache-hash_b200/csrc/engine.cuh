@@ -444,6 +444,10 @@ class Engine final : public kache_table
     Pinned_Buf pin_, pin_ctr_, pin_out_;
     static constexpr int out_depth = 4;     // D2H pieces in flight ahead of the copy-out.
     cudaEvent_t ev_out_[out_depth] = {};
+    static constexpr int out_pieces = 8;    // Pieces of a lookup whose outputs are copied while the next computes.
+    cudaStream_t copy_stream_ = nullptr, in_stream_ = nullptr;
+    cudaEvent_t ev_piece_[out_pieces] = {}, ev_in_[out_pieces] = {};
+    Pinned_Buf pin_piece_;
     Dev_Buf dbatch_, dout_, dretry_a_, dretry_b_, dscan_, dtmp_;
     Dev_Buf dhost_;     // A page-locked host batch's bases and offsets, copied as they lie.
     Dev_Buf dmulti_;    // Several device batches run as one: their descriptors and the merged sequence list.
@@ -470,6 +474,11 @@ class Engine final : public kache_table
     {
         Dev_Batch b{};
         uint64_t total_pos = 0;
+        // Listed on the device in sequence order: seg_off[q] (device) counts the segments of the sequences before q,
+        // so a range of sequences is a range of segments and of output positions. Null where listed otherwise.
+        const uint64_t* seg_off = nullptr;
+        // Set where the bases are still in page-locked host memory here, laid end to end (staged with defer_bases).
+        const char* host_bases = nullptr;
     };
 
     int grid_for(const uint64_t warps_needed, const int warps_per_block) const
@@ -696,7 +705,10 @@ class Engine final : public kache_table
         return static_cast<uint32_t>(s);
     }
 
-    Batch_Info stage_host(const char* const* seqs, const size_t* lens, const size_t n, const bool lanes)
+    // Stages a host batch. With `defer_bases` (a lookup in pieces), a batch laid end to end in page-locked memory is
+    // listed from its offsets alone and its bases are left for the caller to copy (to bi.b.bases), piece by piece;
+    // bi.host_bases is then set.
+    Batch_Info stage_host(const char* const* seqs, const size_t* lens, const size_t n, const bool lanes, const bool defer_bases = false)
     {
         uint64_t bytes = 0, max_pos = 0, all_pos = 0;
         bool contiguous = true;
@@ -725,10 +737,14 @@ class Engine final : public kache_table
             const size_t o_off = (bytes + 64 + 15) / 16 * 16;
             dhost_.ensure(o_off + (n + 1) * 8);
             char* d = dhost_.as<char>();
-            check(cudaMemcpyAsync(d, base, bytes, cudaMemcpyHostToDevice, stream_), "H2D batch");
+            if(!defer_bases)
+                check(cudaMemcpyAsync(d, base, bytes, cudaMemcpyHostToDevice, stream_), "H2D batch");
             check(cudaMemsetAsync(d + bytes, 0, 64, stream_), "memset");
             check(cudaMemcpyAsync(d + o_off, off, (n + 1) * 8, cudaMemcpyHostToDevice, stream_), "H2D offsets");
-            return stage_dev(reinterpret_cast<const uint8_t*>(d), reinterpret_cast<const uint64_t*>(d + o_off), n, lanes);
+            Batch_Info bi = stage_dev(reinterpret_cast<const uint8_t*>(d), reinterpret_cast<const uint64_t*>(d + o_off), n, lanes);
+            if(defer_bases)
+                bi.host_bases = base;
+            return bi;
         }
         if(n >= host_list_max)
             return stage_gathered(seqs, lens, n, bytes, lanes);
@@ -878,6 +894,7 @@ class Engine final : public kache_table
         Batch_Info bi;
         bi.b = Dev_Batch{bases, off, dbatch_.as<uint64_t>(), pos_off, n, nsegs, seg_len};
         bi.total_pos = h[0];
+        bi.seg_off = seg_off;
         return bi;
     }
 
@@ -942,6 +959,7 @@ class Engine final : public kache_table
         Batch_Info bi;
         bi.b = Dev_Batch{bases, off, dbatch_.as<uint64_t>(), pos_off, n, nsegs, seg_len};
         bi.total_pos = total_pos;
+        bi.seg_off = seg_off;
         return bi;
     }
 
@@ -1215,20 +1233,71 @@ class Engine final : public kache_table
 
     // The device address of `bytes` of page-locked host memory at p (one allocation, mapped into the device's address
     // space, as cudaHostAlloc'd memory is on 64-bit systems), or null.
-    static void* mapped(void* p, const size_t bytes)
+    static uint64_t host_bytes(const size_t* lens, const size_t n)
     {
-        if(p == nullptr || bytes == 0)
-            return nullptr;
-        cudaPointerAttributes a{}, z{};
-        if(cudaPointerGetAttributes(&a, p) != cudaSuccess || cudaPointerGetAttributes(&z, static_cast<char*>(p) + bytes - 1) != cudaSuccess)
+        uint64_t b = 0;
+        for(size_t i = 0; i < n; ++i)
+            b += lens[i];
+        return b;
+    }
+
+    bool pinned_range(const void* p, const size_t bytes) const
+    {
+        return p != nullptr && bytes > 0 && pinned(p) && pinned(static_cast<const char*>(p) + bytes - 1);
+    }
+
+    // A lookup in `out_pieces` pieces of sequences (a batch listed in sequence order), each piece's outputs copied to
+    // page-locked host memory on the copy stream once the piece's kernel has run, while the next piece computes.
+    void lookup_pieces(const Batch_Info& bi, uint8_t* d_found, VT* d_val, uint8_t* d_fwd, uint8_t* found, VT* values, uint8_t* fwd)
+    {
+        if(!copy_stream_)
+            check(cudaStreamCreateWithFlags(&copy_stream_, cudaStreamNonBlocking), "cudaStreamCreate");
+        if(!in_stream_)
+            check(cudaStreamCreateWithFlags(&in_stream_, cudaStreamNonBlocking), "cudaStreamCreate");
+        if(!ev_piece_[0])
+            for(int c = 0; c < out_pieces; ++c)
+                check(cudaEventCreateWithFlags(&ev_piece_[c], cudaEventDisableTiming), "event"),
+                check(cudaEventCreateWithFlags(&ev_in_[c], cudaEventDisableTiming), "event");
+        // Piece boundaries at sequences c * n / pieces: their first output position, first segment and first base.
+        const uint64_t n = bi.b.n;
+        pin_piece_.ensure(3 * (out_pieces + 1) * 8);
+        auto* h = pin_piece_.as<uint64_t>();
+        for(int c = 0; c <= out_pieces; ++c)
         {
-            (void)cudaGetLastError();
-            return nullptr;
+            const uint64_t q = n * c / out_pieces;
+            check(cudaMemcpyAsync(h + c, bi.b.pos_off + q, 8, cudaMemcpyDeviceToHost, stream_), "D2H");
+            check(cudaMemcpyAsync(h + out_pieces + 1 + c, bi.seg_off + q, 8, cudaMemcpyDeviceToHost, stream_), "D2H");
+            if(bi.host_bases)
+                check(cudaMemcpyAsync(h + 2 * (out_pieces + 1) + c, bi.b.off + q, 8, cudaMemcpyDeviceToHost, stream_), "D2H");
         }
-        if(a.type != cudaMemoryTypeHost || z.type != cudaMemoryTypeHost || a.devicePointer == nullptr || z.devicePointer == nullptr ||
-           static_cast<char*>(z.devicePointer) - static_cast<char*>(a.devicePointer) != static_cast<ptrdiff_t>(bytes - 1))
-            return nullptr;
-        return a.devicePointer;
+        sync();
+        Lookup_Visitor<set_, VT> vis{T_, bi.b.pos_off, d_found, d_val, d_fwd, 0};
+        for(int c = 0; c < out_pieces; ++c)
+        {
+            const uint64_t p0 = h[c], p1 = h[c + 1], g0 = h[out_pieces + 1 + c], g1 = h[out_pieces + 2 + c];
+            if(bi.host_bases)
+            {
+                // This piece's bases cross on the input stream while the previous piece computes.
+                const uint64_t b0 = h[2 * (out_pieces + 1) + c], b1 = h[2 * (out_pieces + 1) + c + 1];
+                if(b1 > b0)
+                    check(cudaMemcpyAsync(const_cast<uint8_t*>(bi.b.bases) + b0, bi.host_bases + b0, b1 - b0, cudaMemcpyHostToDevice, in_stream_), "H2D batch");
+                check(cudaEventRecord(ev_in_[c], in_stream_), "event record");
+                check(cudaStreamWaitEvent(stream_, ev_in_[c], 0), "event wait");
+            }
+            stream_launch(K_LOOKUP, bi, g0, g1, vis, true);
+            check(cudaEventRecord(ev_piece_[c], stream_), "event record");
+            check(cudaStreamWaitEvent(copy_stream_, ev_piece_[c], 0), "event wait");
+            if(p1 > p0)
+            {
+                check(cudaMemcpyAsync(found + p0, d_found + p0, p1 - p0, cudaMemcpyDeviceToHost, copy_stream_), "D2H");
+                if(d_val)
+                    check(cudaMemcpyAsync(values + p0, d_val + p0, (p1 - p0) * sizeof(VT), cudaMemcpyDeviceToHost, copy_stream_), "D2H");
+                if(d_fwd)
+                    check(cudaMemcpyAsync(fwd + p0, d_fwd + p0, p1 - p0, cudaMemcpyDeviceToHost, copy_stream_), "D2H");
+            }
+        }
+        check(cudaStreamSynchronize(copy_stream_), "cudaStreamSynchronize");
+        sync();
     }
 
     // Copies device output to a host buffer. Into page-locked memory, one copy. Into pageable memory, through pinned
@@ -1309,6 +1378,17 @@ public:
                 cudaEventDestroy(e);
         for(auto& e : tune_ev_)
             cudaEventDestroy(e.first), cudaEventDestroy(e.second);
+        for(int c = 0; c < out_pieces; ++c)
+        {
+            if(ev_piece_[c])
+                cudaEventDestroy(ev_piece_[c]);
+            if(ev_in_[c])
+                cudaEventDestroy(ev_in_[c]);
+        }
+        if(copy_stream_)
+            cudaStreamSynchronize(copy_stream_), cudaStreamDestroy(copy_stream_);
+        if(in_stream_)
+            cudaStreamSynchronize(in_stream_), cudaStreamDestroy(in_stream_);
         if(own_)
             cudaStreamDestroy(own_);
     }
@@ -1376,28 +1456,34 @@ public:
     void lookup(const char* const* seqs, const size_t* lens, size_t n, uint8_t* found, void* values, uint8_t* fwd) override
     {
         std::lock_guard<std::mutex> g(work);
-        const auto bi = stage_host(seqs, lens, n, false);
+        // With outputs in page-locked memory the lookup may run in pieces (below); then the bases of a batch laid end
+        // to end in page-locked memory are copied piece by piece as well.
+        uint64_t P_est = 0;
+        for(size_t i = 0; i < n; ++i)
+            P_est += lens[i] >= size_t(k) ? lens[i] - k + 1 : 0;
+        const size_t vb_est = (!set_ && values) ? sizeof(VT) : 0;
+        const bool out_pinned = P_est > 0 && pinned_range(found, P_est) && (!vb_est || pinned_range(values, P_est * vb_est)) &&
+                                (!fwd || pinned_range(fwd, P_est));
+        const bool pieces = out_pinned && n >= 2 * out_pieces && P_est >= (uint64_t(1) << 22);
+        const auto bi = stage_host(seqs, lens, n, false, pieces);
         const uint64_t P = bi.total_pos;
         const size_t vb = (!set_ && values) ? sizeof(VT) : 0;
-        // Outputs in page-locked memory that the device can address: the kernel writes them there itself, its
-        // stores crossing PCIe while it computes, with no copy after it.
-        if(P > 0)
-        {
-            void* m_found = mapped(found, P);
-            void* m_val = vb ? mapped(values, P * vb) : nullptr;
-            void* m_fwd = fwd ? mapped(fwd, P) : nullptr;
-            if(m_found && (!vb || m_val) && (!fwd || m_fwd))
-            {
-                run_lookup(bi, static_cast<uint8_t*>(m_found), static_cast<VT*>(m_val), static_cast<uint8_t*>(m_fwd));
-                sync();
-                return;
-            }
-        }
         const size_t a_found = (P + 15) / 16 * 16, a_val = (P * vb + 15) / 16 * 16;
         dout_.ensure(a_found + a_val + P + 64);
         uint8_t* d_found = dout_.as<uint8_t>();
         VT* d_val = vb ? reinterpret_cast<VT*>(d_found + a_found) : nullptr;
         uint8_t* d_fwd = fwd ? d_found + a_found + a_val : nullptr;
+        // Outputs in page-locked memory, of a batch listed in sequence order: the lookup runs in pieces of sequences,
+        // each piece's outputs copied by DMA on a second stream while the next piece computes. (The kernel writing
+        // them into mapped host memory itself was measured slower: its 32- and 256-byte stores reach about 33 GB/s
+        // over PCIe, a copy about 55.)
+        if(pieces && bi.seg_off)
+        {
+            lookup_pieces(bi, d_found, d_val, d_fwd, found, static_cast<VT*>(values), fwd);
+            return;
+        }
+        if(bi.host_bases)   // Staged for pieces but not run in them: the bases cross whole first.
+            check(cudaMemcpyAsync(const_cast<uint8_t*>(bi.b.bases), bi.host_bases, bi.b.off ? host_bytes(lens, n) : 0, cudaMemcpyHostToDevice, stream_), "H2D batch");
         run_lookup(bi, d_found, d_val, d_fwd);
         d2h(found, d_found, P);
         if(vb)

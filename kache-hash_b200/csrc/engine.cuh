@@ -708,18 +708,46 @@ class Engine final : public kache_table
     // Stages a host batch. With `defer_bases` (a lookup in pieces), a batch laid end to end in page-locked memory is
     // listed from its offsets alone and its bases are left for the caller to copy (to bi.b.bases), piece by piece;
     // bi.host_bases is then set.
-    Batch_Info stage_host(const char* const* seqs, const size_t* lens, const size_t n, const bool lanes, const bool defer_bases = false)
+    // A host batch's totals, read once: bases, the longest sequence's and all sequences' positions, and whether the
+    // sequences lie end to end. Large batches are summed over the host pool.
+    struct Host_Scan
     {
         uint64_t bytes = 0, max_pos = 0, all_pos = 0;
         bool contiguous = true;
-        for(size_t i = 0; i < n; ++i)
+    };
+
+    Host_Scan scan_host(const char* const* seqs, const size_t* lens, const size_t n) const
+    {
+        constexpr size_t part = size_t(1) << 16;
+        const size_t parts = (n + part - 1) / part;
+        std::vector<Host_Scan> r(std::max<size_t>(parts, 1));
+        parallel_for(parts, 4, [&](const size_t s, const size_t e)
         {
-            bytes += lens[i];
-            const uint64_t np = lens[i] >= size_t(k) ? lens[i] - k + 1 : 0;
-            max_pos = std::max<uint64_t>(max_pos, np), all_pos += np;
-            if(i + 1 < n && seqs[i] + lens[i] != seqs[i + 1])
-                contiguous = false;
-        }
+            for(size_t j = s; j < e; ++j)
+            {
+                Host_Scan& h = r[j];
+                for(size_t i = j * part, i1 = std::min(n, (j + 1) * part); i < i1; ++i)
+                {
+                    h.bytes += lens[i];
+                    const uint64_t np = lens[i] >= size_t(k) ? lens[i] - k + 1 : 0;
+                    h.max_pos = std::max<uint64_t>(h.max_pos, np), h.all_pos += np;
+                    if(i + 1 < n && seqs[i] + lens[i] != seqs[i + 1])
+                        h.contiguous = false;
+                }
+            }
+        });
+        Host_Scan t;
+        for(const auto& h : r)
+            t.bytes += h.bytes, t.max_pos = std::max(t.max_pos, h.max_pos), t.all_pos += h.all_pos, t.contiguous &= h.contiguous;
+        return t;
+    }
+
+    Batch_Info stage_host(const char* const* seqs, const size_t* lens, const size_t n, const bool lanes, const bool defer_bases = false,
+                          const Host_Scan* scanned = nullptr)
+    {
+        const Host_Scan hs = scanned ? *scanned : scan_host(seqs, lens, n);
+        const uint64_t bytes = hs.bytes, max_pos = hs.max_pos, all_pos = hs.all_pos;
+        const bool contiguous = hs.contiguous;
         // Sequences laid end to end in page-locked memory are copied to the device as they lie, with no gather, and
         // listed in segments there (stage_dev): the host only writes the offsets.
         const bool direct = n > 0 && bytes > 0 && contiguous && pinned(seqs[0]) && pinned(seqs[0] + bytes - 1);
@@ -1458,14 +1486,13 @@ public:
         std::lock_guard<std::mutex> g(work);
         // With outputs in page-locked memory the lookup may run in pieces (below); then the bases of a batch laid end
         // to end in page-locked memory are copied piece by piece as well.
-        uint64_t P_est = 0;
-        for(size_t i = 0; i < n; ++i)
-            P_est += lens[i] >= size_t(k) ? lens[i] - k + 1 : 0;
+        const Host_Scan hs = scan_host(seqs, lens, n);
+        const uint64_t P_est = hs.all_pos;
         const size_t vb_est = (!set_ && values) ? sizeof(VT) : 0;
         const bool out_pinned = P_est > 0 && pinned_range(found, P_est) && (!vb_est || pinned_range(values, P_est * vb_est)) &&
                                 (!fwd || pinned_range(fwd, P_est));
         const bool pieces = out_pinned && n >= 2 * out_pieces && P_est >= (uint64_t(1) << 22);
-        const auto bi = stage_host(seqs, lens, n, false, pieces);
+        const auto bi = stage_host(seqs, lens, n, false, pieces, &hs);
         const uint64_t P = bi.total_pos;
         const size_t vb = (!set_ && values) ? sizeof(VT) : 0;
         const size_t a_found = (P + 15) / 16 * 16, a_val = (P * vb + 15) / 16 * 16;

@@ -11,6 +11,7 @@
 
 #include "device_misc.cuh"
 #include "device_lanes.cuh"
+#include "host_copy.hpp"
 #include "kache_b200.h"
 
 #include <cub/device/device_scan.cuh>
@@ -749,7 +750,7 @@ class Engine final : public kache_table
         const uint64_t bytes = hs.bytes, max_pos = hs.max_pos, all_pos = hs.all_pos;
         const bool contiguous = hs.contiguous;
         // Sequences laid end to end in page-locked memory are copied to the device as they lie, with no gather, and
-        // listed in segments there (stage_dev): the host only writes the offsets.
+        // listed in segments there (stage_dev): the host only writes the offsets, in streaming stores (host_copy.hpp).
         const bool direct = n > 0 && bytes > 0 && contiguous && pinned(seqs[0]) && pinned(seqs[0] + bytes - 1);
         if(direct)
         {
@@ -759,7 +760,8 @@ class Engine final : public kache_table
             parallel_for(n, 1 << 16, [&](const size_t s, const size_t e)
             {
                 for(size_t i = s; i < e; ++i)
-                    off[i] = static_cast<uint64_t>(seqs[i] - base);
+                    stream_u64(off + i, static_cast<uint64_t>(seqs[i] - base));
+                stream_fence();
             });
             off[n] = bytes;
             const size_t o_off = (bytes + 64 + 15) / 16 * 16;
@@ -829,9 +831,10 @@ class Engine final : public kache_table
                 i1++;
             parallel_for(i1 - i0, 2048, [&](const size_t s, const size_t e)
             {
+                Stream_Writer w(bases + off[i0 + s]);
                 for(size_t i = i0 + s; i < i0 + e; ++i)
-                    if(lens[i])
-                        std::memcpy(bases + off[i], seqs[i], lens[i]);
+                    w.put(seqs[i], lens[i]);
+                w.finish();
             });
             check(cudaMemcpyAsync(d + o_bases + off[i0], bases + off[i0], off[i1] - off[i0], cudaMemcpyHostToDevice, stream_), "H2D batch");
             i0 = i1;
@@ -870,9 +873,10 @@ class Engine final : public kache_table
                 i1++;
             parallel_for(i1 - i0, 2048, [&](const size_t s, const size_t e)
             {
+                Stream_Writer w(hb + off[i0 + s]);
                 for(size_t i = i0 + s; i < i0 + e; ++i)
-                    if(lens[i])
-                        std::memcpy(hb + off[i], seqs[i], lens[i]);
+                    w.put(seqs[i], lens[i]);
+                w.finish();
             });
             if(off[i1] > off[i0])
                 check(cudaMemcpyAsync(d + off[i0], hb + off[i0], off[i1] - off[i0], cudaMemcpyHostToDevice, stream_), "H2D batch");

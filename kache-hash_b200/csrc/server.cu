@@ -211,14 +211,16 @@ void kache_server::gather(Staged& st)
     src.reserve(n);
     for(const Request* r : g)
         src.insert(src.end(), r->seqs.begin(), r->seqs.end());
+    // Streaming stores: the copy engine reads the staged bases next (host_copy.hpp).
     kache_b200::parallel_for(n, 2048, [&](const size_t s, const size_t e)
     {
+        kache_b200::Stream_Writer w(base + off[s]);
         for(size_t q = s; q < e; ++q)
         {
             st.seqs[q] = base + off[q];
-            if(st.lens[q])
-                std::memcpy(base + off[q], src[q], st.lens[q]);
+            w.put(src[q], st.lens[q]);
         }
+        w.finish();
     });
 }
 

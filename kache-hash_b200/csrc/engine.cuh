@@ -448,6 +448,19 @@ class Engine final : public kache_table
     static constexpr int out_pieces = 8;    // Pieces of a lookup whose outputs are copied while the next computes.
     cudaStream_t copy_stream_ = nullptr, in_stream_ = nullptr;
     cudaEvent_t ev_piece_[out_pieces] = {}, ev_in_[out_pieces] = {};
+    cudaEvent_t ev_stage_ = nullptr, ev_bases_ = nullptr;
+
+    // The copy streams beside the table's stream: input bases cross on in_stream_, outputs return on copy_stream_.
+    void side_streams()
+    {
+        if(!copy_stream_)
+            check(cudaStreamCreateWithFlags(&copy_stream_, cudaStreamNonBlocking), "cudaStreamCreate");
+        if(!in_stream_)
+            check(cudaStreamCreateWithFlags(&in_stream_, cudaStreamNonBlocking), "cudaStreamCreate");
+        if(!ev_stage_)
+            check(cudaEventCreateWithFlags(&ev_stage_, cudaEventDisableTiming), "event"),
+            check(cudaEventCreateWithFlags(&ev_bases_, cudaEventDisableTiming), "event");
+    }
     Pinned_Buf pin_piece_;
     Dev_Buf dbatch_, dout_, dretry_a_, dretry_b_, dscan_, dtmp_;
     Dev_Buf dhost_;     // A page-locked host batch's bases and offsets, copied as they lie.
@@ -767,13 +780,24 @@ class Engine final : public kache_table
             const size_t o_off = (bytes + 64 + 15) / 16 * 16;
             dhost_.ensure(o_off + (n + 1) * 8);
             char* d = dhost_.as<char>();
-            if(!defer_bases)
-                check(cudaMemcpyAsync(d, base, bytes, cudaMemcpyHostToDevice, stream_), "H2D batch");
             check(cudaMemsetAsync(d + bytes, 0, 64, stream_), "memset");
             check(cudaMemcpyAsync(d + o_off, off, (n + 1) * 8, cudaMemcpyHostToDevice, stream_), "H2D offsets");
+            // The bases cross next, on the input stream, while the segments are listed here (host-to-device copies
+            // share a copy engine, so they follow the offsets); the table's stream waits for them before its next
+            // launch.
+            if(!defer_bases)
+            {
+                side_streams();
+                check(cudaEventRecord(ev_stage_, stream_), "event record");
+                check(cudaStreamWaitEvent(in_stream_, ev_stage_, 0), "event wait");
+                check(cudaMemcpyAsync(d, base, bytes, cudaMemcpyHostToDevice, in_stream_), "H2D batch");
+                check(cudaEventRecord(ev_bases_, in_stream_), "event record");
+            }
             Batch_Info bi = stage_dev(reinterpret_cast<const uint8_t*>(d), reinterpret_cast<const uint64_t*>(d + o_off), n, lanes);
             if(defer_bases)
                 bi.host_bases = base;
+            else
+                check(cudaStreamWaitEvent(stream_, ev_bases_, 0), "event wait");
             return bi;
         }
         if(n >= host_list_max)
@@ -1282,10 +1306,7 @@ class Engine final : public kache_table
     // page-locked host memory on the copy stream once the piece's kernel has run, while the next piece computes.
     void lookup_pieces(const Batch_Info& bi, uint8_t* d_found, VT* d_val, uint8_t* d_fwd, uint8_t* found, VT* values, uint8_t* fwd)
     {
-        if(!copy_stream_)
-            check(cudaStreamCreateWithFlags(&copy_stream_, cudaStreamNonBlocking), "cudaStreamCreate");
-        if(!in_stream_)
-            check(cudaStreamCreateWithFlags(&in_stream_, cudaStreamNonBlocking), "cudaStreamCreate");
+        side_streams();
         if(!ev_piece_[0])
             for(int c = 0; c < out_pieces; ++c)
                 check(cudaEventCreateWithFlags(&ev_piece_[c], cudaEventDisableTiming), "event"),
@@ -1303,6 +1324,8 @@ class Engine final : public kache_table
                 check(cudaMemcpyAsync(h + 2 * (out_pieces + 1) + c, bi.b.off + q, 8, cudaMemcpyDeviceToHost, stream_), "D2H");
         }
         sync();
+        if(bi.host_bases)   // The input stream's copies come after this stream's earlier work.
+            check(cudaEventRecord(ev_stage_, stream_), "event record"), check(cudaStreamWaitEvent(in_stream_, ev_stage_, 0), "event wait");
         Lookup_Visitor<set_, VT> vis{T_, bi.b.pos_off, d_found, d_val, d_fwd, 0};
         for(int c = 0; c < out_pieces; ++c)
         {
@@ -1417,6 +1440,8 @@ public:
             if(ev_in_[c])
                 cudaEventDestroy(ev_in_[c]);
         }
+        if(ev_stage_)
+            cudaEventDestroy(ev_stage_), cudaEventDestroy(ev_bases_);
         if(copy_stream_)
             cudaStreamSynchronize(copy_stream_), cudaStreamDestroy(copy_stream_);
         if(in_stream_)

@@ -227,6 +227,32 @@ def run_reference(args):
                       "e2e": {"value": v, "unit": "k-mers/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}))
 
 
+def pcie_floor(d_found, d_vals, t_found, t_vals, d_bases, t_bases, reps=3):
+    """This box's copy floor for the end-to-end step: the find output (found flags and values) copied device to host
+    into the same page-locked buffers, and the find's reads host to device, as plain copies with nothing else running
+    (the fastest of `reps`)."""
+    import torch
+    s = torch.cuda.Stream()
+
+    def once(f):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        with torch.cuda.stream(s):
+            f()
+        s.synchronize()
+        return 1e3 * (time.perf_counter() - t0)
+
+    def out():
+        t_found.copy_(d_found, non_blocking=True)
+        t_vals.copy_(d_vals.view(torch.uint8), non_blocking=True)
+
+    d2h = min(once(out) for _ in range(reps))
+    h2d = min(once(lambda: d_bases.copy_(t_bases, non_blocking=True)) for _ in range(reps))
+    out_bytes = d_found.numel() + d_vals.numel() * d_vals.element_size()
+    return {"d2h_ms": d2h, "d2h_gbs": out_bytes / d2h / 1e6, "h2d_ms": h2d, "h2d_gbs": t_bases.numel() / h2d / 1e6,
+            "form": "the find output device to host and the find's reads host to device, plain copies on this box"}
+
+
 def run_b200(args):
     import torch
     import kache
@@ -360,6 +386,7 @@ def run_b200(args):
 
     # End to end through the C interface with host buffers.
     e2e_ms = e2e_pg_ms = float("nan")
+    pcie = None
     parts_pinned, pg_steps = {}, 0
     if not args.only_dev:
         for _ in range(max(1, args.warmup // 2)):
@@ -383,6 +410,7 @@ def run_b200(args):
             step_e2e(bi, bh, found_pg, vals_pg)
         barrier()
         e2e_pg_ms = max_over_ranks(dist, (time.perf_counter() - t0) * 1000, dev) / pg_steps
+        pcie = pcie_floor(d_found, d_vals, t_f, t_v, d_held_b, keep[1])
 
     if rank == 0:
         line = {
@@ -403,7 +431,8 @@ def run_b200(args):
                     "h2d_bytes_per_step": int(bi.off[-1] + bh.off[-1] + 16 * (bi.n + bh.n)),
                     "d2h_bytes_per_step": int(P_find * 9),
                     "host_buffers": "page-locked (reads and outputs)", "ms_per_call": parts_pinned,
-                    "pageable": {"value": P * ws / (e2e_pg_ms * 1e-3), "ms_per_step": e2e_pg_ms, "steps": pg_steps}},
+                    "pageable": {"value": P * ws / (e2e_pg_ms * 1e-3), "ms_per_step": e2e_pg_ms, "steps": pg_steps},
+                    "pcie_floor": pcie},
             "clocks": clk,
         }
         if ws == 1 and not args.only_dev and not args.no_sub:

@@ -20,8 +20,8 @@ Every rank takes the same collective steps in the same order. for_each is the co
 size is the sum of the shards'.
 
 The shard tables and the describer are given: kache.Table and its describer on the GPU (the default), or any objects
-with their methods. The exchange goes through torch.distributed (NCCL between GPUs, gloo on the CPU) with host
-tensors; with one rank it is the plain table.
+with their methods. The exchange goes through torch.distributed: with NCCL its buffers are staged on this rank's
+current GPU, with gloo they stay in host memory; with one rank it is the plain table.
 """
 import numpy as np
 
@@ -77,6 +77,16 @@ class ShardedTable:
         self.shard = make_shard() if make_shard else kache.Table(k, value_bytes, per, load_factor, pow2, capi=(k == 31))
         self.describe = describe or self.shard.describe
         self.user = self.shard.register()
+        self._device = None
+
+    def _dev(self):
+        """Where the exchange's buffers live: this rank's current GPU under NCCL (which takes device tensors only),
+        else host memory."""
+        import torch
+        if self._device is None:
+            nccl = self.n > 1 and self.dist.get_backend(self.group) == "nccl"
+            self._device = torch.device("cuda", torch.cuda.current_device()) if nccl else torch.device("cpu")
+        return self._device
 
     # ---- Exchange ------------------------------------------------------------------------------------------------
 
@@ -85,24 +95,26 @@ class ShardedTable:
         import torch
         if self.n == 1:
             return [np.asarray(parts[0], dtype=dtype)]
-        sizes = torch.tensor([len(p) for p in parts], dtype=torch.int64)
-        got = torch.empty(self.n, dtype=torch.int64)
+        dev = self._dev()
+        sizes = torch.tensor([len(p) for p in parts], dtype=torch.int64, device=dev)
+        got = torch.empty(self.n, dtype=torch.int64, device=dev)
         self.dist.all_to_all_single(got, sizes, group=self.group)
+        got = got.cpu().numpy()
         # Unsigned 64-bit words travel as signed ones (the bits unchanged): not every backend takes uint64.
         wire = np.int64 if np.dtype(dtype) == np.uint64 else dtype
         flat = np.concatenate([np.asarray(p, dtype=dtype) for p in parts]) if sum(map(len, parts)) else np.zeros(0, dtype)
-        send = torch.from_numpy(np.ascontiguousarray(flat).view(wire))
-        recv = torch.empty(int(got.sum()), dtype=send.dtype)
+        send = torch.from_numpy(np.ascontiguousarray(flat).view(wire)).to(dev)
+        recv = torch.empty(int(got.sum()), dtype=send.dtype, device=dev)
         self.dist.all_to_all_single(recv, send, [int(x) for x in got], [len(p) for p in parts], group=self.group)
-        r = recv.numpy().view(dtype)
-        cuts = np.concatenate([[0], np.cumsum(got.numpy())])
+        r = recv.cpu().numpy().view(dtype)
+        cuts = np.concatenate([[0], np.cumsum(got)])
         return [r[cuts[i]:cuts[i + 1]] for i in range(self.n)]
 
     def _sum(self, x):
         import torch
         if self.n == 1:
             return int(x)
-        t = torch.tensor([int(x)], dtype=torch.int64)
+        t = torch.tensor([int(x)], dtype=torch.int64, device=self._dev())
         self.dist.all_reduce(t, group=self.group)
         return int(t.item())
 

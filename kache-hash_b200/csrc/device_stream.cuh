@@ -51,11 +51,12 @@ struct Row
     uint32_t valid;
 };
 
-__device__ __forceinline__ Row load_row(const uint8_t* seq, const uint64_t len, const uint64_t p, const uint32_t lane)
+// The row at offset o of a segment, through this lane's base pointer sp (the segment's first base + lane) and its
+// bound rem (the sequence's bases from sp on, capped at 2^30): 32-bit arithmetic per row.
+__device__ __forceinline__ Row load_row(const uint8_t* sp, const int32_t rem, const uint32_t o, const uint32_t lane)
 {
     constexpr uint32_t all = 0xFFFFFFFFu;
-    const uint64_t pos = p + lane;
-    const uint32_t ch = pos < len ? seq[pos] : 0u;
+    const uint32_t ch = static_cast<int32_t>(o) < rem ? sp[o] : 0u;
     const uint32_t x = (ch | 0x20u) - 'a';
     const bool ok = x < 20u && ((0x80045u >> x) & 1u);     // a, c, g, t
     const uint32_t code = ((ch >> 2) ^ (ch >> 1)) & 3u;
@@ -129,9 +130,12 @@ __global__ void __launch_bounds__(32 * stream_warps) stream_kernel(const Dev_Bat
         const uint64_t p0 = s * batch.seg_len;
         const uint64_t p1 = min(npos, p0 + batch.seg_len);
         const uint32_t rows = static_cast<uint32_t>((p1 - p0 + 31) / 32);
+        const uint32_t in_seg = static_cast<uint32_t>(p1 - p0);
+        const uint8_t* sp = seq + p0 + lane;
+        const int32_t rem = static_cast<int32_t>(min(len - p0, uint64_t(1) << 30)) - static_cast<int32_t>(lane);
 
-        Row r0 = load_row(seq, len, p0, lane);
-        Row r1 = load_row(seq, len, p0 + 32, lane);
+        Row r0 = load_row(sp, rem, 0, lane);
+        Row r1 = load_row(sp, rem, 32, lane);
         uint64_t hprev;     // This lane's l-mer hash in the newest row hashed.
         {
             uint64_t f, rc;
@@ -144,7 +148,7 @@ __global__ void __launch_bounds__(32 * stream_warps) stream_kernel(const Dev_Bat
         vis.begin_segment(q);
         for(uint32_t r = 0; r < rows; ++r)
         {
-            const Row r2 = load_row(seq, len, p0 + 32 * (r + 2), lane);
+            const Row r2 = load_row(sp, rem, 32 * (r + 2), lane);
             {
                 uint64_t f, rc;
                 window<l>(r1, r2, lane, f, rc);
@@ -158,12 +162,13 @@ __global__ void __launch_bounds__(32 * stream_warps) stream_kernel(const Dev_Bat
             Kmer_Desc d;
             uint64_t f, rc;
             window<k>(r0, r1, lane, f, rc);
-            const uint64_t vbits = ((uint64_t(r1.valid) << 32) | r0.valid) >> lane;
-            const uint64_t km = (k == 32 ? 0xFFFFFFFFull : (1ull << k) - 1);
+            // ACGT flags of the 32 bases from this lane's position on (k <= 32 of them make its k-mer).
+            const uint32_t vbits = __funnelshift_r(r0.valid, r1.valid, lane);
+            constexpr uint32_t km = (k == 32 ? 0xFFFFFFFFu : (1u << k) - 1);
             d.pos = p0 + 32 * r + lane;
             d.out = 0, d.last = false;
             d.q = q;
-            d.in = d.pos < p1;
+            d.in = 32 * r + lane < in_seg;
             d.valid = d.in && (vbits & km) == km;
             d.key = f < rc ? f : rc;
             d.fwd = f <= rc;

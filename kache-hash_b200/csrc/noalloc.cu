@@ -96,9 +96,11 @@ __global__ void __launch_bounds__(32 * stream_warps) noalloc_count_kernel(const 
         const uint64_t p0 = sg * seg_positions;
         const uint64_t p1 = min(npos, p0 + seg_positions);
         const uint32_t rows = static_cast<uint32_t>((p1 - p0 + 31) / 32);
+        const uint8_t* sp = seq + p0 + lane;
+        const int32_t rem = static_cast<int32_t>(min(len - p0, uint64_t(1) << 30)) - static_cast<int32_t>(lane);
 
-        Row r0 = load_row(seq, len, p0, lane);
-        Row r1 = load_row(seq, len, p0 + 32, lane);
+        Row r0 = load_row(sp, rem, 0, lane);
+        Row r1 = load_row(sp, rem, 32, lane);
         {
             uint64_t f, rc;
             window<l>(r0, r1, lane, f, rc);
@@ -107,7 +109,7 @@ __global__ void __launch_bounds__(32 * stream_warps) noalloc_count_kernel(const 
         vis.begin_segment(q);
         for(uint32_t r = 0; r < rows; ++r)
         {
-            const Row r2 = load_row(seq, len, p0 + 32 * (r + 2), lane);
+            const Row r2 = load_row(sp, rem, 32 * (r + 2), lane);
             {
                 uint64_t f, rc;
                 window<l>(r1, r2, lane, f, rc);

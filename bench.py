@@ -303,6 +303,7 @@ def run_b200(args):
         return Batch(v, b.off)
 
     pi, ph = pinned_batch(bi), pinned_batch(bh)
+    t_held = keep[-1]   # The held-out reads' page-locked bases.
     t_f, found_h = pinned(np.zeros(P_find, np.uint8))
     t_v, vals_h = pinned(np.zeros(P_find, np.uint64))
     found_pg, vals_pg = np.zeros(P_find, np.uint8), np.zeros(P_find, np.uint64)
@@ -410,7 +411,7 @@ def run_b200(args):
             step_e2e(bi, bh, found_pg, vals_pg)
         barrier()
         e2e_pg_ms = max_over_ranks(dist, (time.perf_counter() - t0) * 1000, dev) / pg_steps
-        pcie = pcie_floor(d_found, d_vals, t_f, t_v, d_held_b, keep[1])
+        pcie = pcie_floor(d_found, d_vals, t_f, t_v, d_held_b, t_held)
 
     if rank == 0:
         line = {

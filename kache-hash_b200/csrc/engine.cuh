@@ -732,10 +732,10 @@ class Engine final : public kache_table
 
     Host_Scan scan_host(const char* const* seqs, const size_t* lens, const size_t n) const
     {
-        constexpr size_t part = size_t(1) << 16;
+        constexpr size_t part = size_t(1) << 15;
         const size_t parts = (n + part - 1) / part;
         std::vector<Host_Scan> r(std::max<size_t>(parts, 1));
-        parallel_for(parts, 4, [&](const size_t s, const size_t e)
+        parallel_for(parts, 1, [&](const size_t s, const size_t e)
         {
             for(size_t j = s; j < e; ++j)
             {

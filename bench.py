@@ -440,7 +440,8 @@ def run_b200(args):
             # Right after the timed phases, while the GPU's clocks are up (the CPU baseline below leaves it idle).
             line["cold_first_call"] = cold_first_call(dev, stream, d_ins_b.data_ptr(), d_ins_o.data_ptr(), bi.n, d_held_b.data_ptr(),
                                                       d_held_o.data_ptr(), bh.n, d_found.data_ptr(), d_vals.data_ptr(), P)
-        cb = None if args.only_dev else cpu_baseline_sample(ins, held, min(128, os.cpu_count() or 1))
+        # The reference on the host cores, at one GPU only (the other ranks would wait for it).
+        cb = None if (args.only_dev or ws > 1) else cpu_baseline_sample(ins, held, min(128, os.cpu_count() or 1))
         line["cpu_baseline"] = cb
         if ws == 1 and not args.only_dev and not args.no_sub:
             line["config3_batched"] = sub_config3(dev, stream, local)

@@ -323,9 +323,12 @@ inline bool host_acgt(const char c)
 class Seg_Tuner
 {
 public:
-    static constexpr int lens = 4, grids = 4, cands = lens * grids;
+    static constexpr int lens = 4, grids = 3, cands = lens * grids;
     static constexpr uint32_t len[lens] = {16, 32, 64, 128};
-    static constexpr uint32_t blocks[grids] = {16, 8, 4, 2};    // Per SM; the first is the built-in count.
+    // Per SM; the first is the built-in count. Not two: the lane kernels are latency-bound and need their resident
+    // warps (the config-1 upsert took 1.85-1.89 ms at three resident blocks against 1.62-1.67 at four), so two would
+    // only cost each size class a slow exploring call.
+    static constexpr uint32_t blocks[grids] = {16, 8, 4};
 
     static uint32_t seg_len_of(const int c) { return len[c % lens]; }
     static uint32_t blocks_of(const int c) { return blocks[c / lens]; }

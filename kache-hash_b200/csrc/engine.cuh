@@ -366,6 +366,14 @@ class Engine final : public kache_table
     cudaEvent_t ev_piece_[out_pieces] = {}, ev_in_[out_pieces] = {};
     cudaEvent_t ev_stage_ = nullptr, ev_bases_ = nullptr;
 
+    void piece_events()
+    {
+        if(!ev_piece_[0])
+            for(int c = 0; c < out_pieces; ++c)
+                check(cudaEventCreateWithFlags(&ev_piece_[c], cudaEventDisableTiming), "event"),
+                check(cudaEventCreateWithFlags(&ev_in_[c], cudaEventDisableTiming), "event");
+    }
+
     // The copy streams beside the table's stream: input bases cross on in_stream_, outputs return on copy_stream_.
     void side_streams()
     {
@@ -409,6 +417,10 @@ class Engine final : public kache_table
         const uint64_t* seg_off = nullptr;
         // Set where the bases are still in page-locked host memory here, laid end to end (staged with defer_bases).
         const char* host_bases = nullptr;
+        // Set where the bases cross in two halves of sequences (ev_in_[0], ev_in_[1]): the table's stream waits for
+        // the first before any launch, lane launches over segments from half_seg on wait for the second.
+        bool in_halves = false;
+        uint64_t half_seg = 0;
     };
 
     int grid_for(const uint64_t warps_needed, const int warps_per_block) const
@@ -701,19 +713,37 @@ class Engine final : public kache_table
             // The bases cross next, on the input stream, while the segments are listed here (host-to-device copies
             // share a copy engine, so they follow the offsets); the table's stream waits for them before its next
             // launch.
+            // A large batch for the lane kernel crosses in two halves of sequences, so that its first launch need not
+            // wait for the second half (two at most: a half of a 150 bp read set still fills the GPU's lanes).
+            const bool halves = !defer_bases && lanes && n > small_stage_max && bytes >= (size_t(32) << 20);
+            const uint64_t q_half = n / 2, b_half = halves ? off[q_half] : bytes;
             if(!defer_bases)
             {
                 side_streams();
+                piece_events();
                 check(cudaEventRecord(ev_stage_, stream_), "event record");
                 check(cudaStreamWaitEvent(in_stream_, ev_stage_, 0), "event wait");
-                check(cudaMemcpyAsync(d, base, bytes, cudaMemcpyHostToDevice, in_stream_), "H2D batch");
+                check(cudaMemcpyAsync(d, base, b_half, cudaMemcpyHostToDevice, in_stream_), "H2D batch");
+                check(cudaEventRecord(ev_in_[0], in_stream_), "event record");
+                if(bytes > b_half)
+                    check(cudaMemcpyAsync(d + b_half, base + b_half, bytes - b_half, cudaMemcpyHostToDevice, in_stream_), "H2D batch");
                 check(cudaEventRecord(ev_bases_, in_stream_), "event record");
             }
             Batch_Info bi = stage_dev(reinterpret_cast<const uint8_t*>(d), reinterpret_cast<const uint64_t*>(d + o_off), n, lanes);
             if(defer_bases)
+            {
                 bi.host_bases = base;
-            else
-                check(cudaStreamWaitEvent(stream_, ev_bases_, 0), "event wait");
+                return bi;
+            }
+            if(halves && bi.seg_off)
+            {
+                uint64_t* h = pin_ctr_.as<uint64_t>(56);
+                check(cudaMemcpyAsync(h, bi.seg_off + q_half, 8, cudaMemcpyDeviceToHost, stream_), "D2H");
+                sync();
+                bi.half_seg = *h;
+                bi.in_halves = bi.half_seg > 0 && bi.half_seg < bi.b.nsegs;
+            }
+            check(cudaStreamWaitEvent(stream_, bi.in_halves ? ev_in_[0] : ev_bases_, 0), "event wait");
             return bi;
         }
         if(n >= host_list_max)
@@ -943,11 +973,30 @@ class Engine final : public kache_table
     {
         if(se <= sb)
             return;
+        if(bi.in_halves && se > bi.half_seg)
+        {
+            // Segments before half_seg read the first half of the bases, which has crossed; the rest wait for the
+            // second.
+            if(per_position || sb >= bi.half_seg)
+                check(cudaStreamWaitEvent(stream_, ev_bases_, 0), "event wait");
+            else
+            {
+                lane_launch(kind, bi, sb, bi.half_seg, vis);
+                check(cudaStreamWaitEvent(stream_, ev_bases_, 0), "event wait");
+                lane_launch(kind, bi, bi.half_seg, se, vis);
+                return;
+            }
+        }
         if(per_position)
         {
             launch(kind, [&](){ stream_kernel<k, l, Vis><<<grid_for(se - sb, stream_warps), 32 * stream_warps, 0, stream_>>>(bi.b, sb, se, vis); });
             return;
         }
+        lane_launch(kind, bi, sb, se, vis);
+    }
+
+    template <typename Vis> void lane_launch(const uint32_t kind, const Batch_Info& bi, const uint64_t sb, const uint64_t se, const Vis& vis)
+    {
         const bool timed = tune_kind_ >= 0 && tune_cand_ >= 0;
         const uint64_t per_sm = timed ? Seg_Tuner::blocks_of(tune_cand_) : Seg_Tuner::blocks[0];
         const uint64_t blocks = std::min<uint64_t>((se - sb + lane_block - 1) / lane_block, uint64_t(sm_count_) * per_sm);
@@ -1223,10 +1272,7 @@ class Engine final : public kache_table
     void lookup_pieces(const Batch_Info& bi, uint8_t* d_found, VT* d_val, uint8_t* d_fwd, uint8_t* found, VT* values, uint8_t* fwd)
     {
         side_streams();
-        if(!ev_piece_[0])
-            for(int c = 0; c < out_pieces; ++c)
-                check(cudaEventCreateWithFlags(&ev_piece_[c], cudaEventDisableTiming), "event"),
-                check(cudaEventCreateWithFlags(&ev_in_[c], cudaEventDisableTiming), "event");
+        piece_events();
         // Piece boundaries at sequences c * n / pieces: their first output position, first segment and first base.
         const uint64_t n = bi.b.n;
         pin_piece_.ensure(3 * (out_pieces + 1) * 8);

@@ -89,3 +89,42 @@ def test_sharded_table_matches_one_table():
         assert owned and n_own > 0
         shard_sizes += n_own
     assert shard_sizes == O.size()      # every key in exactly one shard
+
+
+def test_cut_runs_edges():
+    """Runs of consecutive valid positions with one owner: none from empty or short sequences or invalid positions,
+    one sequence and one owner each, and together exactly the valid positions, in output order."""
+    sys.path[:0] = [ROOT, os.path.join(ROOT, "kache-hash_b200"), os.path.join(ROOT, "tests")]
+    import kache
+    import sharded
+    k = 31
+    rng = np.random.default_rng(5)
+    seqs = ["", "ACG", "A" * 30, "C" * 31, "ACGT" * 10 + "N" + "TTGCA" * 9, "G" * 35, "N" * 40]
+    b = kache.Batch.of(seqs)
+    P = int(b.positions(k).sum())
+    valid = np.ones(P, bool)
+    start = np.concatenate([[0], np.cumsum(b.positions(k))[:-1]])
+    # Positions whose window holds the N of sequence 4, and every position of the N-only sequence, are not k-mers.
+    n_at = 40
+    for i in range(int(b.positions(k)[4])):
+        if i <= n_at < i + k:
+            valid[start[4] + i] = False
+    valid[start[6]:start[6] + int(b.positions(k)[6])] = False
+    for n in (1, 2, 3):
+        h = rng.integers(0, 2**63, P, dtype=np.uint64)
+        own, seq, p0, cnt, first = sharded.cut_runs(b, k, h, valid, n)
+        covered = np.zeros(P, bool)
+        owners = sharded.owner_of(h, n)
+        for o, q, a, c, f in zip(own, seq, p0, cnt, first):
+            assert c > 0 and f == start[q] + a and a + c <= b.positions(k)[q]
+            assert valid[f:f + c].all() and (owners[f:f + c] == o).all() and not covered[f:f + c].any()
+            covered[f:f + c] = True
+        assert np.array_equal(covered, valid)
+        assert list(first) == sorted(first)
+        # Maximal: the position after a run is invalid, in another sequence, or owned elsewhere.
+        for q, a, c, f in zip(seq, p0, cnt, first):
+            e = f + c
+            if a + c < b.positions(k)[q]:
+                assert not valid[e] or owners[e] != owners[e - 1]
+    z = sharded.cut_runs(kache.Batch.of([]), k, np.zeros(0, np.uint64), np.zeros(0, bool), 2)
+    assert all(len(x) == 0 for x in z)

@@ -429,7 +429,8 @@ def run_b200(args):
                          "peak_source": peak_kind, "kernels": kernels, "random_roof": roof,
                          "model": "A = b_in + b_out + 32*rho + 32*r_slot + 32*w_slot bytes per k-mer; rho from the describer on 5000 reads"},
             "e2e": {"value": P * ws / (e2e_ms * 1e-3), "unit": "k-mers/s", "ms_per_step": e2e_ms,
-                    "h2d_bytes_per_step": int(bi.off[-1] + bh.off[-1] + 16 * (bi.n + bh.n)),
+                    # The reads' bases and the offsets the library lists them by (n + 1 words a batch).
+                    "h2d_bytes_per_step": int(bi.off[-1] + bh.off[-1] + 8 * (bi.n + 1 + bh.n + 1)),
                     "d2h_bytes_per_step": int(P_find * 9),
                     "host_buffers": "page-locked (reads and outputs)", "ms_per_call": parts_pinned,
                     "pageable": {"value": P * ws / (e2e_pg_ms * 1e-3), "ms_per_step": e2e_pg_ms, "steps": pg_steps},
